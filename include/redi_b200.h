@@ -1,0 +1,200 @@
+/*
+ * redi_b200.h — C-ABI of the B200-native Redi neutral-diffusion step.
+ *
+ * Drop-in boundary for the reference's `ocean_redi` module
+ * (JorgeG94/more_benchmarks_dc_ocean, redi/ocean_redi.F90). Two layers:
+ *
+ *  1. A handle API that mirrors the Fortran public interface one to one:
+ *       ocean_redi_t%init / %destroy       -> redi_b200_init / redi_b200_destroy
+ *       redi_calc_coeffs(grid, metrics, eos, this, ms)
+ *                                          -> redi_b200_calc_coeffs
+ *       redi_apply_flux(grid, metrics, this, ms, dt, khtr_u_ext, khtr_v_ext, bc)
+ *                                          -> redi_b200_apply_flux
+ *     The structs mirror the derived types the Fortran passes (hgrid_t,
+ *     ocean_metrics_t, ocean_eos_t, multilayer_cgrid_state_t, ocean_bc_state_t).
+ *     Array arguments are DEVICE pointers (what `!$acc host_data use_device`
+ *     or `c_loc` of a device array yields), column-major with the reference
+ *     shapes. Calls are stream-ordered on `stream` (a cudaStream_t; NULL = the
+ *     legacy default stream) and do not synchronise.
+ *
+ *  2. Exports with the exact signatures of the reference's CUDA launchers
+ *     (redi/opt_kernel.cu:534-549 `redi_opt_launch`, redi/redi_kernel.cu:537-549
+ *     `redi_cuda_launch_`), so the reference's bridge (redi/drivers/redi_bridge.F90)
+ *     and RK2 harness (ideal_benchmark/wrap/rk2_redi.F90) link unchanged.
+ *
+ * Status codes: >= 0 success (REDI_B200_SKIPPED = a reference gate made the call
+ * a no-op, exactly where the Fortran returns early), < 0 error; the message of
+ * the last error on the calling thread is redi_b200_last_error().
+ */
+#ifndef REDI_B200_H
+#define REDI_B200_H
+
+#if defined(__GNUC__)
+#define REDI_B200_API __attribute__((visibility("default")))
+#else
+#define REDI_B200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define REDI_B200_OK 0
+#define REDI_B200_SKIPPED 1
+#define REDI_B200_E_ARG (-1)
+#define REDI_B200_E_STATE (-2)
+#define REDI_B200_E_CUDA (-3)
+#define REDI_B200_E_NOMEM (-4)
+#define REDI_B200_E_UNSUPPORTED (-5)
+
+/* Arithmetic of the step. FP64: bit-identical to the reference with FMA
+ * contraction off. MIXED: FP32 reconstruction / flux arithmetic and compact
+ * coefficient storage, FP64 density differences, slope denominators and
+ * tracer accumulation. */
+#define REDI_B200_FP64 0
+#define REDI_B200_MIXED 1
+
+#define REDI_B200_OBC_WALL 1 /* redi/ocean_boundary_types.F90:14 OBC_WALL */
+
+/* hgrid_t (redi/grid.F90:17-25). */
+typedef struct redi_b200_grid {
+    int nx_total, ny_total; /* cells incl. ghosts: n_phys + 2*nghost */
+    int nx_phys, ny_phys;
+    int nghost;
+    double dx, dy;
+} redi_b200_grid;
+
+/* ocean_metrics_t (redi/ocean_metrics.F90:14-22); device pointers. */
+typedef struct redi_b200_metrics {
+    const double* dy_cu; /* (nx+1, ny) */
+    const double* dx_cv; /* (nx, ny+1) */
+    const double* idxCu; /* (nx+1, ny) */
+    const double* idyCv; /* (nx, ny+1) */
+    const double* areaT; /* (nx, ny)   */
+    const double* wet_u; /* (nx+1, ny) */
+    const double* wet_v; /* (nx, ny+1) */
+} redi_b200_metrics;
+
+/* ocean_eos_t, LINEAR variant (redi/ocean_eos.F90:239-278). variant must be 0
+ * (EOS_VARIANT_LINEAR), the only variant any Redi configuration reaches. */
+typedef struct redi_b200_eos {
+    int variant;
+    double rho0, T_ref, S_ref, alpha_T, beta_S;
+} redi_b200_eos;
+
+/* multilayer_cgrid_state_t (redi/multilayer_cgrid_state.F90:18-28).
+ * idx_temperature / idx_salinity are 1-based indices into hTr (0 = not
+ * registered), as in the Fortran. hTr is a HOST array of ntracers DEVICE
+ * pointers, each an (nx, ny, nz_ml) thickness-weighted tracer. */
+typedef struct redi_b200_state {
+    int nz_ml;
+    int idx_temperature, idx_salinity;
+    int ntracers;
+    const double* h_layer; /* (nx, ny, nz_ml), k=1 the bed */
+    double* const* hTr;
+} redi_b200_state;
+
+/* ocean_bc_state_t (redi/ocean_boundary_types.F90:20-24): bc_type per edge. */
+typedef struct redi_b200_bc {
+    int west, east, south, north;
+} redi_b200_bc;
+
+/* Device pointers of the Phase-A coefficient slots held by a handle
+ * (ocean_redi_t%uPoL ... %vhEff, ocean_redi.F90:105-110), FP64 handles only. */
+typedef struct redi_b200_coeffs {
+    double *uPoL, *uPoR, *uhEff;
+    int *uKoL, *uKoR;
+    double *vPoL, *vPoR, *vhEff;
+    int *vKoL, *vKoR;
+    double *khtr_u, *khtr_v;
+    int nsurf;
+} redi_b200_coeffs;
+
+typedef struct redi_b200 redi_b200; /* ocean_redi_t */
+
+/* ocean_redi_init (ocean_redi.F90:466-507): allocate the coefficient slots for
+ * grid%nx_total x grid%ny_total x nz_ml (nz_ml < 1 is taken as 1) and set them
+ * to the inert state (Po = 0, Ko = 1, hEff = 0). Fails with E_UNSUPPORTED where
+ * the reference's init `error stop`s (the column is longer than the kernels
+ * support). The new handle has enable = 0 and khtr = 0, like the Fortran. */
+REDI_B200_API int redi_b200_init(const redi_b200_grid* grid, int nz_ml, int precision, redi_b200** out);
+
+/* ocean_redi_destroy (ocean_redi.F90:509-529). NULL is accepted. */
+REDI_B200_API int redi_b200_destroy(redi_b200* self);
+
+/* ocean_redi_t%enable, %khtr (ocean_redi.F90:78-87). */
+REDI_B200_API int redi_b200_set_enable(redi_b200* self, int enable);
+REDI_B200_API int redi_b200_set_khtr(redi_b200* self, double khtr);
+
+/* redi_calc_coeffs (ocean_redi.F90:572-607). */
+REDI_B200_API int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
+                          redi_b200* self, const redi_b200_state* ms, void* stream);
+
+/* redi_apply_flux (ocean_redi.F90:927-1002). khtr_u_ext / khtr_v_ext (device,
+ * (nx+1,ny) / (nx,ny+1)) are optional: both non-NULL selects the per-face path,
+ * otherwise the scalar khtr is broadcast. bc may be NULL (all edges WALL).
+ * Every tracer of ms is updated, all in one fused pass. */
+REDI_B200_API int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* metrics, redi_b200* self,
+                         const redi_b200_state* ms, double dt, const double* khtr_u_ext, const double* khtr_v_ext,
+                         const redi_b200_bc* bc, void* stream);
+
+/* Device pointers of the handle's coefficient slots. */
+REDI_B200_API int redi_b200_get_coeffs(const redi_b200* self, redi_b200_coeffs* out);
+
+/* Bytes of device scratch the handle holds beside its coefficient slots. */
+REDI_B200_API long long redi_b200_workspace_bytes(const redi_b200* self);
+
+/* Message of the last error on the calling thread ("" if none). */
+REDI_B200_API const char* redi_b200_last_error(void);
+
+/* Library version: major*10000 + minor*100 + patch. */
+REDI_B200_API int redi_b200_version(void);
+
+/* Instrumentation (no counterpart in the reference). Kernel ids are
+ * 0 column_state, 1 neutral_sweep, 2 tracer_recon, 3 cell_update,
+ * 4 mixed_recon, 5 mixed_cell_update, 6 mixed_sweep, 7 domain_persistent,
+ * 8 auxiliary; redi_b200_kernel_count() is their number.
+ * redi_b200_launch_count(k) counts launches of kernel k since load (k < 0:
+ * all). Between profile_begin and profile_end every launch is bracketed by a
+ * CUDA event pair on its own stream; profile_end waits for them and returns,
+ * per kernel id, the summed device time (ms) and the number of launches. */
+REDI_B200_API int redi_b200_kernel_count(void);
+REDI_B200_API unsigned long long redi_b200_launch_count(int kernel);
+REDI_B200_API int redi_b200_profile_begin(void);
+REDI_B200_API int redi_b200_profile_end(double* total_ms, unsigned long long* counts, int n);
+
+/* Same signature, argument meaning and launch sequence as the reference's
+ * optimized launcher (redi/opt_kernel.cu:534-574): Phase A into the caller's
+ * u/v slots, khtr_u/v = khtr_*_ext, then Phase B for T (t_htr) and S (s_htr);
+ * synchronises the device before returning. All arrays are device pointers,
+ * all scalars by reference (Fortran default). tr_snap is accepted and not
+ * written (the fused Phase B reads pre-step tracers from its own scratch).
+ * Like the reference it returns nothing: argument errors are reported through
+ * redi_b200_last_error() and stderr, and no kernel is launched. */
+REDI_B200_API void redi_opt_launch(const int* nx, const int* ny, const int* nz, const int* ns, const double* dt,
+                     const int* nghost, const int* nxp, const int* nyp, const int* ww, const int* we,
+                     const int* wsz, const int* wn, const double* rho0, const double* T_ref, const double* S_ref,
+                     const double* alpha_T, const double* beta_S, const double* h_layer, double* t_htr,
+                     double* s_htr, const double* wet_u, const double* wet_v, double* uPoL, double* uPoR,
+                     int* uKoL, int* uKoR, double* uhEff, double* vPoL, double* vPoR, int* vKoL, int* vKoR,
+                     double* vhEff, const double* khtr_u_ext, const double* khtr_v_ext, double* khtr_u,
+                     double* khtr_v, const double* dy_cu, const double* dx_cv, const double* idxCu,
+                     const double* idyCv, const double* areaT, double* tr_snap);
+
+/* The reference's faithful launcher name (redi/redi_kernel.cu:537-549); same
+ * behaviour as redi_opt_launch (the two reference launchers are bit-identical). */
+REDI_B200_API void redi_cuda_launch_(const int* nx, const int* ny, const int* nz, const int* ns, const double* dt,
+                       const int* nghost, const int* nxp, const int* nyp, const int* ww, const int* we,
+                       const int* wsz, const int* wn, const double* rho0, const double* T_ref, const double* S_ref,
+                       const double* alpha_T, const double* beta_S, const double* h_layer, double* t_htr,
+                       double* s_htr, const double* wet_u, const double* wet_v, double* uPoL, double* uPoR,
+                       int* uKoL, int* uKoR, double* uhEff, double* vPoL, double* vPoR, int* vKoL, int* vKoR,
+                       double* vhEff, const double* khtr_u_ext, const double* khtr_v_ext, double* khtr_u,
+                       double* khtr_v, const double* dy_cu, const double* dx_cv, const double* idxCu,
+                       const double* idyCv, const double* areaT, double* tr_snap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* REDI_B200_H */

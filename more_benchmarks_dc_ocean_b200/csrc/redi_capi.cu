@@ -1,0 +1,532 @@
+// C-ABI of the B200 Redi step (include/redi_b200.h): the ocean_redi_t handle,
+// the reference's gates and argument checks, scratch management and the
+// reference-compatible launcher exports.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/redi_b200.h"
+#include "redi_kernels.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(REDI_B200_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+bool aligned(const T* p) {
+    return (reinterpret_cast<uintptr_t>(p) % alignof(T)) == 0;
+}
+
+__global__ void k_fill(double* p, size_t n, double v) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t < n) p[t] = v;
+}
+__global__ void k_fill_int(int* p, size_t n, int v) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t < n) p[t] = v;
+}
+
+cudaError_t fill(double* p, size_t n, double v, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_fill<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, v);
+    return cudaGetLastError();
+}
+cudaError_t fill_int(int* p, size_t n, int v, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_fill_int<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, v);
+    return cudaGetLastError();
+}
+
+// Grow-only device scratch.
+struct Scratch {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int device = -1;
+    cudaError_t reserve(size_t need) {
+        if (need <= bytes) return cudaSuccess;
+        if (ptr) {
+            cudaError_t e = cudaFree(ptr);
+            ptr = nullptr;
+            bytes = 0;
+            if (e != cudaSuccess) return e;
+        }
+        cudaError_t e = cudaMalloc(&ptr, need);
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            return e;
+        }
+        bytes = need;
+        return cudaSuccess;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+bool dims_ok(int nx, int ny, int nz, std::string& why) {
+    if (nx < 1 || ny < 1) { why = "nx_total and ny_total must be >= 1"; return false; }
+    if (nz < 1) { why = "nz must be >= 1"; return false; }
+    if (nz > redi::kNzMax) {
+        why = "nz = " + std::to_string(nz) + " exceeds the supported maximum of " + std::to_string(redi::kNzMax) +
+              " layers (the reference's init stops for 2*nz+2 > NZ_STACK_MAX in the same way)";
+        return false;
+    }
+    const long long ns = 2LL * nz + 2;
+    if ((long long)(nx + 1) * (ny + 1) * ns >= (1LL << 31)) { why = "domain too large for 32-bit face indexing"; return false; }
+    return true;
+}
+
+// Phase A on FP64 slots with caller-provided or handle-owned arrays.
+int run_plain_phase_a(int nx, int ny, int nz, const redi::EosLin& eos, const double* h, const double* th,
+                      const double* sh, const double* wet_u, const double* wet_v, const redi::FaceOut& u,
+                      const redi::FaceOut& v, Scratch& ws, cudaStream_t st) {
+    cudaError_t e = ws.reserve(redi::plain_phase_a_scratch(nx, ny, nz));
+    if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (phase A)");
+    const size_t nifc = (size_t)nx * ny * (nz + 1);
+    redi::ColumnStateArgs cs{};
+    cs.nx = nx; cs.ny = ny; cs.nz = nz; cs.eos = eos;
+    cs.h = h; cs.th = th; cs.sh = sh;
+    cs.ifc = reinterpret_cast<redi::IfcState*>(ws.ptr);
+    cs.pint = reinterpret_cast<double*>(cs.ifc + nifc);
+    redi::SweepArgs sw{};
+    sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos.rho0;
+    sw.wet_u = wet_u; sw.wet_v = wet_v; sw.ifc = cs.ifc; sw.pint = cs.pint;
+    sw.u = u; sw.v = v;
+    e = redi::launch_plain_phase_a(cs, sw, st);
+    if (e != cudaSuccess) return cuda_fail(e, "phase A launch");
+    return REDI_B200_OK;
+}
+
+struct PhaseBInputs {
+    int nx, ny, nz, nghost, nxp, nyp;
+    int walls[4];
+    double dt, khtr;
+    const double *khtr_u, *khtr_v, *dy_cu, *dx_cv, *idxCu, *idyCv, *areaT, *h;
+    redi::FaceIn u, v;
+};
+
+int run_plain_phase_b(const PhaseBInputs& in, int ntr, double* const* htr, Scratch& ws, cudaStream_t st) {
+    const int group = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
+    cudaError_t e = ws.reserve(redi::plain_phase_b_scratch(in.nx, in.ny, in.nz, group));
+    if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (phase B)");
+    const size_t ncol = (size_t)in.nx * in.ny;
+    for (int t0 = 0; t0 < ntr; t0 += group) {
+        const int nt = (ntr - t0) < group ? (ntr - t0) : group;
+        redi::ReconArgs rc{};
+        rc.nx = in.nx; rc.ny = in.ny; rc.nz = in.nz; rc.ntr = nt; rc.h = in.h;
+        rc.ti = reinterpret_cast<double*>(ws.ptr);
+        rc.ppm = reinterpret_cast<redi::PpmLayer*>(rc.ti + (size_t)nt * ncol * (in.nz + 1));
+        redi::CellUpdateArgs cu{};
+        cu.nx = in.nx; cu.ny = in.ny; cu.nz = in.nz; cu.ntr = nt;
+        cu.nghost = in.nghost; cu.nxp = in.nxp; cu.nyp = in.nyp;
+        cu.wall_w = in.walls[0]; cu.wall_e = in.walls[1]; cu.wall_s = in.walls[2]; cu.wall_n = in.walls[3];
+        cu.dt = in.dt; cu.khtr = in.khtr; cu.khtr_u = in.khtr_u; cu.khtr_v = in.khtr_v;
+        cu.dy_cu = in.dy_cu; cu.dx_cv = in.dx_cv; cu.idxCu = in.idxCu; cu.idyCv = in.idyCv; cu.areaT = in.areaT;
+        cu.u = in.u; cu.v = in.v; cu.ti = rc.ti; cu.ppm = rc.ppm;
+        for (int n = 0; n < nt; ++n) {
+            rc.htr[n] = htr[t0 + n];
+            cu.htr[n] = htr[t0 + n];
+        }
+        e = redi::launch_plain_phase_b(rc, cu, st);
+        if (e != cudaSuccess) return cuda_fail(e, "phase B launch");
+    }
+    return REDI_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Launch counter and optional per-kernel event timing.
+// ---------------------------------------------------------------------------
+struct Profiler {
+    std::mutex mu;
+    bool active = false;
+    struct Rec { int kid; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    unsigned long long launches[redi::K_NUM] = {};
+    cudaEvent_t take() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+};
+Profiler g_prof;
+
+}  // namespace
+
+namespace redi {
+void launch_begin(int kid, cudaStream_t st) {
+    std::lock_guard<std::mutex> lock(g_prof.mu);
+    __atomic_add_fetch(&g_prof.launches[kid], 1ULL, __ATOMIC_RELAXED);
+    if (!g_prof.active) return;
+    Profiler::Rec r{kid, g_prof.take(), nullptr};
+    cudaEventRecord(r.a, st);
+    g_prof.recs.push_back(r);
+}
+void launch_end(int kid, cudaStream_t st) {
+    std::lock_guard<std::mutex> lock(g_prof.mu);
+    if (!g_prof.active) return;
+    for (auto it = g_prof.recs.rbegin(); it != g_prof.recs.rend(); ++it) {
+        if (it->kid == kid && it->b == nullptr) {
+            it->b = g_prof.take();
+            cudaEventRecord(it->b, st);
+            return;
+        }
+    }
+}
+}  // namespace redi
+
+// ---------------------------------------------------------------------------
+// ocean_redi_t
+// ---------------------------------------------------------------------------
+struct redi_b200 {
+    bool is_init = false;
+    bool enable = false;
+    bool continuous = true;
+    double khtr = 0.0;
+    double ref_pres = -1.0;
+    int nx_total = 0, ny_total = 0, nz_ml = 0, nsurf = 0;
+    int precision = REDI_B200_FP64;
+    int device = -1;
+    // FP64 coefficient slots (ocean_redi.F90:105-116).
+    double *uPoL = nullptr, *uPoR = nullptr, *uhEff = nullptr;
+    int *uKoL = nullptr, *uKoR = nullptr;
+    double *vPoL = nullptr, *vPoR = nullptr, *vhEff = nullptr;
+    int *vKoL = nullptr, *vKoR = nullptr;
+    double *khtr_u = nullptr, *khtr_v = nullptr;
+    Scratch ws;
+    std::vector<void*> allocations;
+
+    cudaError_t alloc(void** p, size_t bytes) {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) allocations.push_back(*p);
+        return e;
+    }
+    void free_all() {
+        for (void* p : allocations) cudaFree(p);
+        allocations.clear();
+        ws.release();
+    }
+};
+
+extern "C" {
+
+int redi_b200_version(void) { return 100; }
+
+int redi_b200_kernel_count(void) { return redi::K_NUM; }
+
+unsigned long long redi_b200_launch_count(int kernel) {
+    if (kernel < 0) {
+        unsigned long long t = 0;
+        for (int k = 0; k < redi::K_NUM; ++k) t += __atomic_load_n(&g_prof.launches[k], __ATOMIC_RELAXED);
+        return t;
+    }
+    if (kernel >= redi::K_NUM) return 0;
+    return __atomic_load_n(&g_prof.launches[kernel], __ATOMIC_RELAXED);
+}
+
+int redi_b200_profile_begin(void) {
+    std::lock_guard<std::mutex> lock(g_prof.mu);
+    for (auto& r : g_prof.recs) {
+        g_prof.pool.push_back(r.a);
+        if (r.b) g_prof.pool.push_back(r.b);
+    }
+    g_prof.recs.clear();
+    g_prof.active = true;
+    return REDI_B200_OK;
+}
+
+int redi_b200_profile_end(double* total_ms, unsigned long long* counts, int n) {
+    std::lock_guard<std::mutex> lock(g_prof.mu);
+    g_prof.active = false;
+    if (!total_ms || !counts || n < redi::K_NUM) return fail(REDI_B200_E_ARG, "redi_b200_profile_end: output arrays too small");
+    for (int k = 0; k < n; ++k) { total_ms[k] = 0.0; counts[k] = 0; }
+    for (auto& r : g_prof.recs) {
+        if (!r.b) continue;
+        cudaError_t e = cudaEventSynchronize(r.b);
+        if (e != cudaSuccess) return cuda_fail(e, "redi_b200_profile_end");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        total_ms[r.kid] += ms;
+        counts[r.kid] += 1;
+    }
+    return REDI_B200_OK;
+}
+
+const char* redi_b200_last_error(void) { return g_last_error.c_str(); }
+
+int redi_b200_init(const redi_b200_grid* grid, int nz_ml, int precision, redi_b200** out) {
+    if (!out) return fail(REDI_B200_E_ARG, "redi_b200_init: out is NULL");
+    *out = nullptr;
+    if (!grid) return fail(REDI_B200_E_ARG, "redi_b200_init: grid is NULL");
+    if (precision != REDI_B200_FP64 && precision != REDI_B200_MIXED)
+        return fail(REDI_B200_E_ARG, "redi_b200_init: precision must be REDI_B200_FP64 or REDI_B200_MIXED");
+    int nz = nz_ml < 1 ? 1 : nz_ml;  // ocean_redi.F90:478-480
+    std::string why;
+    if (!dims_ok(grid->nx_total, grid->ny_total, nz, why)) {
+        return fail(nz > redi::kNzMax ? REDI_B200_E_UNSUPPORTED : REDI_B200_E_ARG, "redi_b200_init: " + why);
+    }
+    if (precision == REDI_B200_MIXED)
+        return fail(REDI_B200_E_UNSUPPORTED, "redi_b200_init: the mixed-precision form is not built in this library");
+    redi_b200* s = new (std::nothrow) redi_b200();
+    if (!s) return fail(REDI_B200_E_NOMEM, "redi_b200_init: host allocation failed");
+    cudaGetDevice(&s->device);
+    const int nx = grid->nx_total, ny = grid->ny_total, ns = 2 * nz + 2;
+    s->nx_total = nx; s->ny_total = ny; s->nz_ml = nz; s->nsurf = ns; s->precision = precision;
+    const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = s->alloc(p, bytes); };
+    A((void**)&s->uPoL, nu * ns * 8); A((void**)&s->uPoR, nu * ns * 8); A((void**)&s->uhEff, nu * (ns - 1) * 8);
+    A((void**)&s->uKoL, nu * ns * 4); A((void**)&s->uKoR, nu * ns * 4);
+    A((void**)&s->vPoL, nv * ns * 8); A((void**)&s->vPoR, nv * ns * 8); A((void**)&s->vhEff, nv * (ns - 1) * 8);
+    A((void**)&s->vKoL, nv * ns * 4); A((void**)&s->vKoR, nv * ns * 4);
+    A((void**)&s->khtr_u, nu * 8); A((void**)&s->khtr_v, nv * 8);
+    if (e != cudaSuccess) {
+        s->free_all();
+        delete s;
+        return fail(REDI_B200_E_NOMEM, std::string("redi_b200_init: device allocation failed: ") + cudaGetErrorString(e));
+    }
+    // ocean_redi.F90:493-505: Po = 0, Ko = 1, hEff = 0, khtr_* = 0.
+    cudaStream_t st = 0;
+    cudaMemsetAsync(s->uPoL, 0, nu * ns * 8, st); cudaMemsetAsync(s->uPoR, 0, nu * ns * 8, st);
+    cudaMemsetAsync(s->uhEff, 0, nu * (ns - 1) * 8, st);
+    cudaMemsetAsync(s->vPoL, 0, nv * ns * 8, st); cudaMemsetAsync(s->vPoR, 0, nv * ns * 8, st);
+    cudaMemsetAsync(s->vhEff, 0, nv * (ns - 1) * 8, st);
+    fill_int(s->uKoL, nu * ns, 1, st); fill_int(s->uKoR, nu * ns, 1, st);
+    fill_int(s->vKoL, nv * ns, 1, st); fill_int(s->vKoR, nv * ns, 1, st);
+    cudaMemsetAsync(s->khtr_u, 0, nu * 8, st);
+    cudaMemsetAsync(s->khtr_v, 0, nv * 8, st);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        s->free_all();
+        delete s;
+        return cuda_fail(e, "redi_b200_init");
+    }
+    s->is_init = true;
+    *out = s;
+    g_last_error.clear();
+    return REDI_B200_OK;
+}
+
+int redi_b200_destroy(redi_b200* s) {
+    if (!s) return REDI_B200_OK;
+    s->is_init = false;
+    s->free_all();
+    delete s;
+    return REDI_B200_OK;
+}
+
+int redi_b200_set_enable(redi_b200* s, int enable) {
+    if (!s) return fail(REDI_B200_E_ARG, "redi_b200_set_enable: handle is NULL");
+    s->enable = enable != 0;
+    return REDI_B200_OK;
+}
+
+int redi_b200_set_khtr(redi_b200* s, double khtr) {
+    if (!s) return fail(REDI_B200_E_ARG, "redi_b200_set_khtr: handle is NULL");
+    s->khtr = khtr;
+    return REDI_B200_OK;
+}
+
+int redi_b200_get_coeffs(const redi_b200* s, redi_b200_coeffs* out) {
+    if (!s || !out) return fail(REDI_B200_E_ARG, "redi_b200_get_coeffs: NULL argument");
+    if (s->precision != REDI_B200_FP64)
+        return fail(REDI_B200_E_STATE, "redi_b200_get_coeffs: mixed-precision handles keep packed coefficients");
+    out->uPoL = s->uPoL; out->uPoR = s->uPoR; out->uhEff = s->uhEff; out->uKoL = s->uKoL; out->uKoR = s->uKoR;
+    out->vPoL = s->vPoL; out->vPoR = s->vPoR; out->vhEff = s->vhEff; out->vKoL = s->vKoL; out->vKoR = s->vKoR;
+    out->khtr_u = s->khtr_u; out->khtr_v = s->khtr_v; out->nsurf = s->nsurf;
+    return REDI_B200_OK;
+}
+
+long long redi_b200_workspace_bytes(const redi_b200* s) { return s ? (long long)s->ws.bytes : 0; }
+
+int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
+                          redi_b200* s, const redi_b200_state* ms, void* stream) {
+    if (!grid || !metrics || !eos || !s || !ms) return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: NULL argument");
+    // Gates of ocean_redi.F90:585-593.
+    if (!s->is_init) return REDI_B200_SKIPPED;
+    if (!s->enable) return REDI_B200_SKIPPED;
+    if (ms->idx_temperature <= 0 || ms->idx_salinity <= 0) return REDI_B200_SKIPPED;
+    if (!ms->h_layer) return REDI_B200_SKIPPED;
+    const int nx = grid->nx_total, ny = grid->ny_total, nz = ms->nz_ml;
+    if (s->nz_ml != nz) return REDI_B200_SKIPPED;
+    if (nx != s->nx_total || ny != s->ny_total)
+        return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: grid extents differ from the handle's");
+    if (eos->variant != 0) return fail(REDI_B200_E_UNSUPPORTED, "redi_b200_calc_coeffs: only the LINEAR EOS is supported");
+    if (ms->idx_temperature > ms->ntracers || ms->idx_salinity > ms->ntracers || !ms->hTr)
+        return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: temperature/salinity index outside the tracer table");
+    const double* th = ms->hTr[ms->idx_temperature - 1];
+    const double* sh = ms->hTr[ms->idx_salinity - 1];
+    if (!th || !sh || !metrics->wet_u || !metrics->wet_v)
+        return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: NULL device array");
+    if (!aligned(ms->h_layer) || !aligned(th) || !aligned(sh) || !aligned(metrics->wet_u) || !aligned(metrics->wet_v))
+        return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: misaligned device array");
+    redi::EosLin e{eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    redi::FaceOut u{s->uPoL, s->uPoR, s->uKoL, s->uKoR, s->uhEff};
+    redi::FaceOut v{s->vPoL, s->vPoR, s->vKoL, s->vKoR, s->vhEff};
+    return run_plain_phase_a(nx, ny, nz, e, ms->h_layer, th, sh, metrics->wet_u, metrics->wet_v, u, v, s->ws, st);
+}
+
+int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* metrics, redi_b200* s,
+                         const redi_b200_state* ms, double dt, const double* khtr_u_ext, const double* khtr_v_ext,
+                         const redi_b200_bc* bc, void* stream) {
+    if (!grid || !metrics || !s || !ms) return fail(REDI_B200_E_ARG, "redi_b200_apply_flux: NULL argument");
+    // Gates of ocean_redi.F90:951-959.
+    if (!s->is_init) return REDI_B200_SKIPPED;
+    if (!s->enable) return REDI_B200_SKIPPED;
+    if (!ms->h_layer) return REDI_B200_SKIPPED;
+    if (!ms->hTr || ms->ntracers <= 0) return REDI_B200_SKIPPED;
+    const int nx = grid->nx_total, ny = grid->ny_total, nz = ms->nz_ml;
+    if (s->nz_ml != nz) return REDI_B200_SKIPPED;
+    if (nx != s->nx_total || ny != s->ny_total)
+        return fail(REDI_B200_E_ARG, "redi_b200_apply_flux: grid extents differ from the handle's");
+    // ocean_redi.F90:964-973: walls default closed.
+    int walls[4] = {1, 1, 1, 1};
+    if (bc) {
+        walls[0] = bc->west == REDI_B200_OBC_WALL;
+        walls[1] = bc->east == REDI_B200_OBC_WALL;
+        walls[2] = bc->south == REDI_B200_OBC_WALL;
+        walls[3] = bc->north == REDI_B200_OBC_WALL;
+    }
+    const bool use_ext = khtr_u_ext && khtr_v_ext;  // :975
+    if (!use_ext && s->khtr <= 0.0) return REDI_B200_SKIPPED;  // :978
+    const double* need[] = {metrics->dy_cu, metrics->dx_cv, metrics->idxCu, metrics->idyCv, metrics->areaT};
+    for (const double* p : need)
+        if (!p || !aligned(p)) return fail(REDI_B200_E_ARG, "redi_b200_apply_flux: NULL or misaligned metric array");
+    for (int t = 0; t < ms->ntracers; ++t)
+        if (!ms->hTr[t] || !aligned(ms->hTr[t]))
+            return fail(REDI_B200_E_ARG, "redi_b200_apply_flux: NULL or misaligned tracer " + std::to_string(t + 1));
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
+    // Resolve the per-face KhTr into the slots (:981-987).
+    cudaError_t e;
+    if (use_ext) {
+        e = cudaMemcpyAsync(s->khtr_u, khtr_u_ext, nu * 8, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s->khtr_v, khtr_v_ext, nv * 8, cudaMemcpyDeviceToDevice, st);
+    } else {
+        e = fill(s->khtr_u, nu, s->khtr, st);
+        if (e == cudaSuccess) e = fill(s->khtr_v, nv, s->khtr, st);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "redi_b200_apply_flux: khtr resolve");
+    PhaseBInputs in{};
+    in.nx = nx; in.ny = ny; in.nz = nz; in.nghost = grid->nghost; in.nxp = grid->nx_phys; in.nyp = grid->ny_phys;
+    for (int w = 0; w < 4; ++w) in.walls[w] = walls[w];
+    in.dt = dt; in.khtr = s->khtr; in.khtr_u = s->khtr_u; in.khtr_v = s->khtr_v;
+    in.dy_cu = metrics->dy_cu; in.dx_cv = metrics->dx_cv; in.idxCu = metrics->idxCu; in.idyCv = metrics->idyCv;
+    in.areaT = metrics->areaT; in.h = ms->h_layer;
+    in.u = redi::FaceIn{s->uPoL, s->uPoR, s->uKoL, s->uKoR, s->uhEff};
+    in.v = redi::FaceIn{s->vPoL, s->vPoR, s->vKoL, s->vKoR, s->vhEff};
+    return run_plain_phase_b(in, ms->ntracers, ms->hTr, s->ws, st);
+}
+
+// ---------------------------------------------------------------------------
+// Reference-compatible launchers (redi/opt_kernel.cu:534-574,
+// redi/redi_kernel.cu:537-580).
+// ---------------------------------------------------------------------------
+static std::mutex g_compat_mu;
+static std::vector<Scratch> g_compat_ws;  // one per device
+
+static void compat_launch(const char* name, const int* nx_, const int* ny_, const int* nz_, const int* ns_,
+                          const double* dt_, const int* nghost_, const int* nxp_, const int* nyp_, const int* ww_,
+                          const int* we_, const int* wsz_, const int* wn_, const double* rho0_, const double* T_ref_,
+                          const double* S_ref_, const double* alpha_T_, const double* beta_S_, const double* h_layer,
+                          double* t_htr, double* s_htr, const double* wet_u, const double* wet_v, double* uPoL,
+                          double* uPoR, int* uKoL, int* uKoR, double* uhEff, double* vPoL, double* vPoR, int* vKoL,
+                          int* vKoR, double* vhEff, const double* khtr_u_ext, const double* khtr_v_ext,
+                          double* khtr_u, double* khtr_v, const double* dy_cu, const double* dx_cv,
+                          const double* idxCu, const double* idyCv, const double* areaT) {
+    auto report = [&](int code, const std::string& msg) {
+        fail(code, std::string(name) + ": " + msg);
+        std::fprintf(stderr, "%s: %s\n", name, msg.c_str());
+    };
+    const void* scalars[] = {nx_, ny_, nz_, ns_, dt_, nghost_, nxp_, nyp_, ww_, we_, wsz_, wn_,
+                             rho0_, T_ref_, S_ref_, alpha_T_, beta_S_};
+    for (const void* p : scalars)
+        if (!p) { report(REDI_B200_E_ARG, "NULL scalar argument"); return; }
+    const int nx = *nx_, ny = *ny_, nz = *nz_, ns = *ns_;
+    std::string why;
+    if (!dims_ok(nx, ny, nz, why)) { report(REDI_B200_E_ARG, why); return; }
+    if (ns != 2 * nz + 2) { report(REDI_B200_E_ARG, "ns must equal 2*nz+2"); return; }
+    const void* arrays[] = {h_layer, t_htr, s_htr, wet_u, wet_v, uPoL, uPoR, uKoL, uKoR, uhEff, vPoL, vPoR,
+                            vKoL, vKoR, vhEff, khtr_u_ext, khtr_v_ext, khtr_u, khtr_v, dy_cu, dx_cv, idxCu,
+                            idyCv, areaT};
+    for (const void* p : arrays)
+        if (!p || (reinterpret_cast<uintptr_t>(p) % 4) != 0) { report(REDI_B200_E_ARG, "NULL or misaligned array"); return; }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_compat_mu);
+    if ((int)g_compat_ws.size() <= dev) g_compat_ws.resize(dev + 1);
+    Scratch& ws = g_compat_ws[dev];
+    cudaStream_t st = 0;  // the reference launches on the legacy default stream
+    redi::EosLin e{*rho0_, *T_ref_, *S_ref_, *alpha_T_, *beta_S_};
+    redi::FaceOut u{uPoL, uPoR, uKoL, uKoR, uhEff}, v{vPoL, vPoR, vKoL, vKoR, vhEff};
+    int rc = run_plain_phase_a(nx, ny, nz, e, h_layer, t_htr, s_htr, wet_u, wet_v, u, v, ws, st);
+    if (rc < 0) { report(rc, g_last_error); return; }
+    const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
+    cudaMemcpyAsync(khtr_u, khtr_u_ext, nu * 8, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(khtr_v, khtr_v_ext, nv * 8, cudaMemcpyDeviceToDevice, st);
+    PhaseBInputs in{};
+    in.nx = nx; in.ny = ny; in.nz = nz; in.nghost = *nghost_; in.nxp = *nxp_; in.nyp = *nyp_;
+    in.walls[0] = *ww_; in.walls[1] = *we_; in.walls[2] = *wsz_; in.walls[3] = *wn_;
+    in.dt = *dt_; in.khtr = 0.0; in.khtr_u = khtr_u; in.khtr_v = khtr_v;
+    in.dy_cu = dy_cu; in.dx_cv = dx_cv; in.idxCu = idxCu; in.idyCv = idyCv; in.areaT = areaT; in.h = h_layer;
+    in.u = redi::FaceIn{uPoL, uPoR, uKoL, uKoR, uhEff};
+    in.v = redi::FaceIn{vPoL, vPoR, vKoL, vKoR, vhEff};
+    double* trs[2] = {t_htr, s_htr};
+    rc = run_plain_phase_b(in, 2, trs, ws, st);
+    if (rc < 0) { report(rc, g_last_error); return; }
+    cudaDeviceSynchronize();
+}
+
+void redi_opt_launch(const int* nx, const int* ny, const int* nz, const int* ns, const double* dt, const int* nghost,
+                     const int* nxp, const int* nyp, const int* ww, const int* we, const int* wsz, const int* wn,
+                     const double* rho0, const double* T_ref, const double* S_ref, const double* alpha_T,
+                     const double* beta_S, const double* h_layer, double* t_htr, double* s_htr, const double* wet_u,
+                     const double* wet_v, double* uPoL, double* uPoR, int* uKoL, int* uKoR, double* uhEff,
+                     double* vPoL, double* vPoR, int* vKoL, int* vKoR, double* vhEff, const double* khtr_u_ext,
+                     const double* khtr_v_ext, double* khtr_u, double* khtr_v, const double* dy_cu,
+                     const double* dx_cv, const double* idxCu, const double* idyCv, const double* areaT,
+                     double* tr_snap) {
+    (void)tr_snap;
+    compat_launch("redi_opt_launch", nx, ny, nz, ns, dt, nghost, nxp, nyp, ww, we, wsz, wn, rho0, T_ref, S_ref,
+                  alpha_T, beta_S, h_layer, t_htr, s_htr, wet_u, wet_v, uPoL, uPoR, uKoL, uKoR, uhEff, vPoL, vPoR,
+                  vKoL, vKoR, vhEff, khtr_u_ext, khtr_v_ext, khtr_u, khtr_v, dy_cu, dx_cv, idxCu, idyCv, areaT);
+}
+
+void redi_cuda_launch_(const int* nx, const int* ny, const int* nz, const int* ns, const double* dt,
+                       const int* nghost, const int* nxp, const int* nyp, const int* ww, const int* we,
+                       const int* wsz, const int* wn, const double* rho0, const double* T_ref, const double* S_ref,
+                       const double* alpha_T, const double* beta_S, const double* h_layer, double* t_htr,
+                       double* s_htr, const double* wet_u, const double* wet_v, double* uPoL, double* uPoR,
+                       int* uKoL, int* uKoR, double* uhEff, double* vPoL, double* vPoR, int* vKoL, int* vKoR,
+                       double* vhEff, const double* khtr_u_ext, const double* khtr_v_ext, double* khtr_u,
+                       double* khtr_v, const double* dy_cu, const double* dx_cv, const double* idxCu,
+                       const double* idyCv, const double* areaT, double* tr_snap) {
+    (void)tr_snap;
+    compat_launch("redi_cuda_launch_", nx, ny, nz, ns, dt, nghost, nxp, nyp, ww, we, wsz, wn, rho0, T_ref, S_ref,
+                  alpha_T, beta_S, h_layer, t_htr, s_htr, wet_u, wet_v, uPoL, uPoR, uKoL, uKoR, uhEff, vPoL,
+                  vPoR, vKoL, vKoR, vhEff, khtr_u_ext, khtr_v_ext, khtr_u, khtr_v, dy_cu, dx_cv, idxCu, idyCv,
+                  areaT);
+}
+
+}  // extern "C"

@@ -1,0 +1,541 @@
+// Plain FP64 Redi neutral-diffusion step for sm_100a.
+//
+// Compiled with FMA contraction off (-fmad=false): every FP64 operation is the
+// reference's (redi/ocean_redi.F90), in the reference's order, so results are
+// bit-identical to the CPU oracle and to the reference's own CUDA ports built
+// the same way.
+//
+// Decomposition (one column = all nz layers of one (i,j) T-cell):
+//
+//   Phase A  redi_calc_coeffs (ocean_redi.F90:572-812)
+//     k_column_state   one thread per column: top-down PPM interface T, S
+//                      (thickness geometry shared by T and S), hydrostatic
+//                      interface pressure and the EOS derivatives, written once
+//                      per column. The reference rebuilds each column for each
+//                      of its up to four faces.
+//     k_neutral_sweep  one thread per interior wet face: the 2nz+2-surface
+//                      continuous sweep (ocean_redi.F90:307-464) over the two
+//                      prebuilt columns, writing PoL/PoR/KoL/KoR/hEff in the
+//                      reference layout (coalesced: neighbouring threads are
+//                      neighbouring faces along i).
+//
+//   Phase B  redi_apply_flux (ocean_redi.F90:927-1181), all tracers fused
+//     k_tracer_recon   one thread per (column, tracer group): top-down PPM
+//                      tracer edges + limiter (ocean_redi.F90:852-891), written
+//                      once per column and tracer. The reference rebuilds each
+//                      column 8 times per cell (5 in its hoisted variant).
+//     k_cell_update    one thread per T-cell column: the four faces W, E, S, N
+//                      in the reference order, sublayers ks = 1..ns-1 in order,
+//                      accumulating into the cell's own dTr exactly as
+//                      redi_apply_flux_impl does, then hTr += dTr * (1/areaT).
+//                      Coefficients are read once for every tracer of the group.
+//
+// Layouts: cell fields (nx, ny, nz) column-major (i fastest); face fields as in
+// the reference ((nx+1, ny, ns) u, (nx, ny+1, ns) v). Scratch: per-column
+// interface records [column][interface] so each thread streams its own
+// column(s) through L1.
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "redi_device.cuh"
+#include "redi_kernels.h"
+
+namespace redi {
+namespace plain {
+
+// ---------------------------------------------------------------------------
+// Streaming top-down PPM interface reconstruction (redi_interface_scalar,
+// ocean_redi.F90:231-254) of NS scalars that share one thickness column.
+//
+// Layers are pulled from the surface down through `load(t, h, s)`, t = 1..nk
+// top-down; edge(t) needs layers t-2..t+1, so a four-layer register window
+// replaces the reference's column arrays. `emit(t, e, s_above)` receives
+// interface t (1..nk+1), its NS edge values, and the NS means of the layer
+// just above it (layer t-1; undefined for t = 1).
+// ---------------------------------------------------------------------------
+template <int NS, class Load, class Emit>
+__device__ __forceinline__ void stream_edges(int nk, Load load, Emit emit) {
+    double hA = 0.0, hB, hC, hD = 0.0;  // h(t-2), h(t-1), h(t), h(t+1)
+    double sB[NS], sC[NS], sD[NS];      // layer scalars t-1, t, t+1
+    double dB[NS], dC[NS];              // PLM slopes of layers t-1, t
+    double e[NS];
+
+    // t = 1: edge(1) = tr(1) - 0.5*diff(1), diff(1) = 0.
+    load(1, hC, sC);
+    if (nk >= 2) load(2, hD, sD);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        dC[n] = 0.0;
+        e[n] = sC[n] - 0.5 * dC[n];
+        sB[n] = 0.0;
+    }
+    emit(1, e, sB);
+
+    for (int t = 2; t <= nk; ++t) {
+        // shift the window down one layer: (t-1) <- t, t <- t+1
+        hA = (t >= 3) ? hB : hA;
+        hB = hC;
+        hC = hD;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            sB[n] = sC[n];
+            sC[n] = sD[n];
+            dB[n] = dC[n];
+        }
+        if (t + 1 <= nk) load(t + 1, hD, sD);
+        // diff(t): PLM slope for 2 <= t <= nk-1, PCM (0) at t = nk.
+        if (t <= nk - 1) {
+            const PlmGeom pg = plm_geom(hB, hC, hD);
+#pragma unroll
+            for (int n = 0; n < NS; ++n) dC[n] = plm_slope(pg, sB[n], sC[n], sD[n]);
+        } else {
+#pragma unroll
+            for (int n = 0; n < NS; ++n) dC[n] = 0.0;
+        }
+        const double hkm1 = (t >= 3) ? hA : hB;   // h(max(1, t-2))
+        const double hkp2 = (t + 1 <= nk) ? hD : hC;  // h(min(nk, t+1))
+        const EdgeGeom eg = edge_geom(hkm1, hB, hC, hkp2, kHNeglect);
+#pragma unroll
+        for (int n = 0; n < NS; ++n) e[n] = ppm_edge(eg, sB[n], sC[n], dB[n], dC[n]);
+        emit(t, e, sB);
+    }
+    // edge(nk+1) = tr(nk) + 0.5*diff(nk), diff(nk) = 0.
+#pragma unroll
+    for (int n = 0; n < NS; ++n) e[n] = sC[n] + 0.5 * dC[n];
+    emit(nk + 1, e, sC);
+}
+
+// ---------------------------------------------------------------------------
+// Phase A, step 1: per-column interface state (redi_build_column,
+// ocean_redi.F90:609-654).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a) {
+    const int ncol = a.nx * a.ny;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int nz = a.nz;
+    const double* __restrict__ h = a.h + col;
+    const double* __restrict__ th = a.th + col;
+    const double* __restrict__ sh = a.sh + col;
+    IfcState* __restrict__ ifc = a.ifc + (size_t)col * (nz + 1);
+    double* __restrict__ pint = a.pint + (size_t)col * (nz + 1);
+
+    const EosLin eos = a.eos;
+    const double dsv_dt = eos.alpha_T / (eos.rho0 * eos.rho0);  // ocean_eos.F90:511
+    const double dsv_ds = -eos.beta_S / (eos.rho0 * eos.rho0);  // ocean_eos.F90:512
+    const double grho = kGravity * eos.rho0;
+    double P = 0.0;
+    double h_layer_above = 0.0;
+
+    auto load = [&](int t, double& hv, double (&sv)[2]) {
+        const size_t off = (size_t)(nz - t) * ncol;  // native k = nz+1-t (1-based)
+        const double hk = __ldg(h + off);
+        const double he = fmax(hk, kHDivEps);
+        hv = hk;
+        sv[0] = __ldg(th + off) / he;
+        sv[1] = __ldg(sh + off) / he;
+    };
+    auto emit = [&](int t, const double (&e)[2], const double (&)[2]) {
+        if (t >= 2) P = P + grho * h_layer_above;  // Pint(t) = Pint(t-1) + g*rho0*h(t-1)
+        const double rho_i = eos.rho0 + eos.beta_S * (e[1] - eos.S_ref) - eos.alpha_T * (e[0] - eos.T_ref);
+        IfcState s;
+        s.T = e[0];
+        s.S = e[1];
+        s.dRdT = -(rho_i * rho_i) * dsv_dt;
+        s.dRdS = -(rho_i * rho_i) * dsv_ds;
+        double2* q = reinterpret_cast<double2*>(ifc + (t - 1));
+        q[0] = make_double2(s.T, s.S);
+        q[1] = make_double2(s.dRdT, s.dRdS);
+        pint[t - 1] = P;
+        if (t <= nz) h_layer_above = __ldg(h + (size_t)(nz - t) * ncol);
+    };
+    stream_edges<2>(nz, load, emit);
+}
+
+// ---------------------------------------------------------------------------
+// Phase A, step 2: the continuous neutral-surface sweep per face
+// (redi_neutral_positions_continuous + redi_face_coeffs, ocean_redi.F90:307-464,
+// 656-692) and the slot writes of redi_calc_coeffs_x/_y (:694-812).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
+    const int dir = blockIdx.y;  // 0: u-faces, 1: v-faces
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int colL, colR, fo, nface;
+    size_t fstride;
+    if (dir == 0) {  // Fortran faces i = 2..nx, j = 1..ny
+        nface = (nx - 1) * ny;
+        if (t >= nface) return;
+        const int j = t / (nx - 1), fi = 1 + t % (nx - 1);
+        colL = (fi - 1) + nx * j;
+        colR = fi + nx * j;
+        fo = fi + (nx + 1) * j;
+        fstride = (size_t)(nx + 1) * ny;
+    } else {  // Fortran faces j = 2..ny, i = 1..nx
+        nface = nx * (ny - 1);
+        if (t >= nface) return;
+        const int fj = 1 + t / nx, i = t % nx;
+        colL = i + nx * (fj - 1);
+        colR = i + nx * fj;
+        fo = i + nx * fj;
+        fstride = (size_t)nx * (ny + 1);
+    }
+    const FaceOut o = dir == 0 ? a.u : a.v;
+    double* __restrict__ PoL = o.PoL + fo;
+    double* __restrict__ PoR = o.PoR + fo;
+    int* __restrict__ KoL = o.KoL + fo;
+    int* __restrict__ KoR = o.KoR + fo;
+    double* __restrict__ hEff = o.hEff + fo;
+    const double wet = __ldg((dir == 0 ? a.wet_u : a.wet_v) + fo);
+
+    if (!(wet > 0.0)) {  // ocean_redi.F90:722-730: inert coefficients
+        for (int s = 0; s < ns; ++s) {
+            PoL[s * fstride] = 0.0;
+            PoR[s * fstride] = 0.0;
+            KoL[s * fstride] = 1;
+            KoR[s * fstride] = 1;
+        }
+        for (int s = 0; s < ns - 1; ++s) hEff[s * fstride] = 0.0;
+        return;
+    }
+
+    const IfcState* __restrict__ L = a.ifc + (size_t)colL * (nz + 1);
+    const IfcState* __restrict__ R = a.ifc + (size_t)colR * (nz + 1);
+    const double* __restrict__ Pl = a.pint + (size_t)colL * (nz + 1);
+    const double* __restrict__ Pr = a.pint + (size_t)colR * (nz + 1);
+    const double pa_to_h = 1.0 / (kGravity * a.rho0);
+    const int nk = nz;
+
+    int kr = 1, kl = 1;
+    double lastP_right = 0.0, lastP_left = 0.0;
+    int lastK_right = 1, lastK_left = 1;
+    bool reached_bottom = false, search_left = false, search_right = false;
+    double absL_prev = 0.0, absR_prev = 0.0;
+
+    for (int ks = 1; ks <= ns; ++ks) {
+        int klm1 = max(kl - 1, 1);
+        int krm1 = max(kr - 1, 1);
+        const IfcState Lk = load_ifc(L + (kl - 1));
+        const IfcState Rk = load_ifc(R + (kr - 1));
+        const double dRho = secant_drho(Rk, Lk);
+        if (!reached_bottom) {
+            if (dRho < 0.0) {
+                search_left = true;
+                search_right = false;
+            } else if (dRho > 0.0) {
+                search_right = true;
+                search_left = false;
+            } else if (kl + kr == 2) {
+                search_left = true;
+                search_right = false;
+            } else {
+                search_left = !search_left;
+                search_right = !search_right;
+            }
+        }
+        double pol, por;
+        int kol, kor;
+        if (search_left) {
+            const IfcState La = load_ifc(L + (klm1 - 1)), Lb = load_ifc(L + klm1);
+            const double dRhoTop = secant_drho(La, Rk);
+            const double dRhoBot = secant_drho(Lb, Rk);
+            if (dRhoTop > 0.0 || kr + kl == 2) pol = 0.0;
+            else if (dRhoTop >= dRhoBot) pol = 1.0;
+            else pol = interpolate_position(dRhoTop, __ldg(Pl + klm1 - 1), dRhoBot, __ldg(Pl + klm1));
+            if (pol >= 1.0 && klm1 < nk) {
+                klm1 += 1;
+                pol = pol - 1.0;
+            }
+            if ((double)(klm1 - lastK_left) + (pol - lastP_left) < 0.0) {
+                pol = lastP_left;
+                klm1 = lastK_left;
+            }
+            kol = klm1;
+            if (kr <= nk) { por = 0.0; kor = kr; }
+            else          { por = 1.0; kor = nk; }
+            if (kr <= nk) kr += 1;
+            else { reached_bottom = true; search_right = true; search_left = false; }
+        } else {  // search_right (exactly one direction is always set)
+            const IfcState Ra = load_ifc(R + (krm1 - 1)), Rb = load_ifc(R + krm1);
+            const double dRhoTop = secant_drho(Ra, Lk);
+            const double dRhoBot = secant_drho(Rb, Lk);
+            if (dRhoTop >= 0.0 || kr + kl == 2) por = 0.0;
+            else if (dRhoTop >= dRhoBot) por = 1.0;
+            else por = interpolate_position(dRhoTop, __ldg(Pr + krm1 - 1), dRhoBot, __ldg(Pr + krm1));
+            if (por >= 1.0 && krm1 < nk) {
+                krm1 += 1;
+                por = por - 1.0;
+            }
+            if ((double)(krm1 - lastK_right) + (por - lastP_right) < 0.0) {
+                por = lastP_right;
+                krm1 = lastK_right;
+            }
+            kor = krm1;
+            if (kl <= nk) { pol = 0.0; kol = kl; }
+            else          { pol = 1.0; kol = nk; }
+            if (kl <= nk) kl += 1;
+            else { reached_bottom = true; search_right = false; search_left = true; }
+        }
+        lastK_left = kol;
+        lastP_left = pol;
+        lastK_right = kor;
+        lastP_right = por;
+        const size_t so = (size_t)(ks - 1) * fstride;
+        PoL[so] = pol;
+        PoR[so] = por;
+        KoL[so] = kol;
+        KoR[so] = kor;
+        // redi_absolute_position (ocean_redi.F90:289-298) and the harmonic-mean
+        // effective thickness (:452-462), then Pa -> m (:688-691).
+        const double pl0 = __ldg(Pl + kol - 1), pl1 = __ldg(Pl + kol);
+        const double pr0 = __ldg(Pr + kor - 1), pr1 = __ldg(Pr + kor);
+        const double absL = pl0 + pol * (pl1 - pl0);
+        const double absR = pr0 + por * (pr1 - pr0);
+        if (ks > 1) {
+            const double hL = absL - absL_prev;
+            const double hR = absR - absR_prev;
+            double he = 0.0;
+            if (hL + hR > 0.0) he = 2.0 * hL * hR / (hL + hR);
+            hEff[so - fstride] = he * pa_to_h;
+        }
+        absL_prev = absL;
+        absR_prev = absR;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phase B, step 1: per-column tracer reconstruction for a group of NT tracers
+// (redi_tracer_column, ocean_redi.F90:852-891). Writes, per tracer and
+// column, the nz+1 interface values Tint and the nz prepared PPM layers.
+// ---------------------------------------------------------------------------
+template <int NT>
+__global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
+    const int ncol = a.nx * a.ny;
+    const int ngroups = (a.ntr + NT - 1) / NT;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= ncol * ngroups) return;
+    const int col = gid % ncol;
+    const int g = gid / ncol;
+    const int tr0 = g * NT;
+    const int nt = min(NT, a.ntr - tr0);
+    const int nz = a.nz;
+    const double* __restrict__ h = a.h + col;
+    const double* htr[NT];
+    double* ti[NT];
+    PpmLayer* ppm[NT];
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        const int tr = tr0 + (n < nt ? n : 0);
+        htr[n] = a.htr[tr] + col;
+        ti[n] = a.ti + (size_t)tr * ncol * (nz + 1) + (size_t)col * (nz + 1);
+        ppm[n] = a.ppm + (size_t)tr * ncol * nz + (size_t)col * nz;
+    }
+    double e_prev[NT];
+
+    auto load = [&](int t, double& hv, double (&sv)[NT]) {
+        const size_t off = (size_t)(nz - t) * ncol;
+        const double hk = __ldg(h + off);
+        const double he = fmax(hk, kHDivEps);
+        hv = hk;
+#pragma unroll
+        for (int n = 0; n < NT; ++n) sv[n] = __ldg(htr[n] + off) / he;
+    };
+    auto emit = [&](int t, const double (&e)[NT], const double (&s_above)[NT]) {
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            if (n < nt) {
+                ti[n][t - 1] = e[n];
+                if (t >= 2) {  // layer t-1 is complete: limit its edges
+                    double alk = e_prev[n], ark = e[n];
+                    const double tlk = s_above[n];
+                    ppm_limit(alk, ark, tlk);
+                    const PpmLayer q = make_ppm_layer(alk, ark, tlk);
+                    double2* p = reinterpret_cast<double2*>(ppm[n] + (t - 2));
+                    p[0] = make_double2(q.aL, q.dA);
+                    p[1] = make_double2(q.a6o3, q.B);
+                }
+            }
+            e_prev[n] = e[n];
+        }
+    };
+    stream_edges<NT>(nz, load, emit);
+}
+
+// ---------------------------------------------------------------------------
+// Phase B, step 2: per-cell flux divergence (redi_apply_flux_impl +
+// redi_face_flux + redi_sublayer_dT, ocean_redi.F90:893-925, 1037-1181).
+// ---------------------------------------------------------------------------
+struct SurfInterp {  // tracer values at one neutral surface, both columns
+    double tl, tr;
+};
+
+template <int NT>
+__device__ __forceinline__ void face_accumulate(const CellUpdateArgs& a, int nt, int tr0, const FaceIn& F,
+                                                size_t fo, size_t fstride, int colL, int colR, double coef,
+                                                bool is_left, double (&dTr)[NT][kNzMax]) {
+    const int nz = a.nz, ns = 2 * nz + 2;
+    const int ncol = a.nx * a.ny;
+    const double* tiL[NT];
+    const double* tiR[NT];
+    const PpmLayer* pL[NT];
+    const PpmLayer* pR[NT];
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        const int tr = tr0 + (n < nt ? n : 0);
+        tiL[n] = a.ti + (size_t)tr * ncol * (nz + 1) + (size_t)colL * (nz + 1);
+        tiR[n] = a.ti + (size_t)tr * ncol * (nz + 1) + (size_t)colR * (nz + 1);
+        pL[n] = a.ppm + (size_t)tr * ncol * nz + (size_t)colL * nz;
+        pR[n] = a.ppm + (size_t)tr * ncol * nz + (size_t)colR * nz;
+    }
+    const double* __restrict__ hEff = F.hEff + fo;
+    const double* __restrict__ PoL = F.PoL + fo;
+    const double* __restrict__ PoR = F.PoR + fo;
+    const int* __restrict__ KoL = F.KoL + fo;
+    const int* __restrict__ KoR = F.KoR + fo;
+
+    int cached = -1;  // surface whose interpolated tracer values are held in `top`
+    int kl_top = 1, kr_top = 1;
+    double pl_top = 0.0, pr_top = 0.0;
+    SurfInterp top[NT];
+
+    for (int s = 0; s < ns - 1; ++s) {
+        const double he = __ldg(hEff + s * fstride);
+        if (he == 0.0) continue;
+        if (cached != s) {
+            kl_top = min(max(__ldg(KoL + s * fstride), 1), nz);
+            kr_top = min(max(__ldg(KoR + s * fstride), 1), nz);
+            pl_top = __ldg(PoL + s * fstride);
+            pr_top = __ldg(PoR + s * fstride);
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                top[n].tl = (1.0 - pl_top) * __ldg(tiL[n] + kl_top - 1) + pl_top * __ldg(tiL[n] + kl_top);
+                top[n].tr = (1.0 - pr_top) * __ldg(tiR[n] + kr_top - 1) + pr_top * __ldg(tiR[n] + kr_top);
+            }
+        }
+        const int kl_bot = min(max(__ldg(KoL + (s + 1) * fstride), 1), nz);
+        const int kr_bot = min(max(__ldg(KoR + (s + 1) * fstride), 1), nz);
+        const double pl_bot = __ldg(PoL + (s + 1) * fstride);
+        const double pr_bot = __ldg(PoR + (s + 1) * fstride);
+        const double xRl = pl_bot + (double)(kl_bot - kl_top);
+        const double xRr = pr_bot + (double)(kr_bot - kr_top);
+        const int knat = is_left ? nz - kl_top : nz - kr_top;
+        SurfInterp bot[NT];
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            bot[n].tl = (1.0 - pl_bot) * __ldg(tiL[n] + kl_bot - 1) + pl_bot * __ldg(tiL[n] + kl_bot);
+            bot[n].tr = (1.0 - pr_bot) * __ldg(tiR[n] + kr_bot - 1) + pr_bot * __ldg(tiR[n] + kr_bot);
+            if (n < nt) {
+                const double tlay = ppm_ave(pl_top, xRl, load_ppm(pL[n] + kl_top - 1));
+                const double trlay = ppm_ave(pr_top, xRr, load_ppm(pR[n] + kr_top - 1));
+                const double dT = guarded_dT(top[n].tr - top[n].tl, bot[n].tr - bot[n].tl, trlay - tlay);
+                const double flx = dT * he * coef;
+                if (is_left) dTr[n][knat] = dTr[n][knat] + flx;
+                else         dTr[n][knat] = dTr[n][knat] - flx;
+            }
+            top[n] = bot[n];
+        }
+        cached = s + 1;
+        kl_top = kl_bot;
+        kr_top = kr_bot;
+        pl_top = pl_bot;
+        pr_top = pr_bot;
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(128) k_cell_update(CellUpdateArgs a, int tr0) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    const int ncol = nx * ny;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= ncol) return;
+    const int nt = min(NT, a.ntr - tr0);
+    const int i = col % nx, j = col / nx;
+    const int I = i + 1, J = j + 1;  // Fortran indices
+    const int wuf_w = a.nghost + 1, wuf_e = a.nghost + a.nxp + 1;
+    const int wvf_s = a.nghost + 1, wvf_n = a.nghost + a.nyp + 1;
+
+    double dTr[NT][kNzMax];
+#pragma unroll
+    for (int n = 0; n < NT; ++n)
+        for (int k = 0; k < nz; ++k) dTr[n][k] = 0.0;
+
+    const size_t ustride = (size_t)(nx + 1) * ny, vstride = (size_t)nx * (ny + 1);
+    // WEST u-face (face I): this cell is the RIGHT column.
+    if (I >= 2 && !((a.wall_w && I == wuf_w) || (a.wall_e && I == wuf_e))) {
+        const size_t f = (size_t)i + (size_t)(nx + 1) * j;
+        const double kh = a.khtr_u ? __ldg(a.khtr_u + f) : a.khtr;
+        const double coef = a.dt * kh * __ldg(a.dy_cu + f) * __ldg(a.idxCu + f);
+        face_accumulate<NT>(a, nt, tr0, a.u, f, ustride, col - 1, col, coef, false, dTr);
+    }
+    // EAST u-face (face I+1): this cell is the LEFT column.
+    if (I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e))) {
+        const size_t f = (size_t)(i + 1) + (size_t)(nx + 1) * j;
+        const double kh = a.khtr_u ? __ldg(a.khtr_u + f) : a.khtr;
+        const double coef = a.dt * kh * __ldg(a.dy_cu + f) * __ldg(a.idxCu + f);
+        face_accumulate<NT>(a, nt, tr0, a.u, f, ustride, col, col + 1, coef, true, dTr);
+    }
+    // SOUTH v-face (face J): this cell is the RIGHT (north) column.
+    if (J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n))) {
+        const size_t f = (size_t)i + (size_t)nx * j;
+        const double kh = a.khtr_v ? __ldg(a.khtr_v + f) : a.khtr;
+        const double coef = a.dt * kh * __ldg(a.dx_cv + f) * __ldg(a.idyCv + f);
+        face_accumulate<NT>(a, nt, tr0, a.v, f, vstride, col - nx, col, coef, false, dTr);
+    }
+    // NORTH v-face (face J+1): this cell is the LEFT (south) column.
+    if (J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))) {
+        const size_t f = (size_t)i + (size_t)nx * (j + 1);
+        const double kh = a.khtr_v ? __ldg(a.khtr_v + f) : a.khtr;
+        const double coef = a.dt * kh * __ldg(a.dx_cv + f) * __ldg(a.idyCv + f);
+        face_accumulate<NT>(a, nt, tr0, a.v, f, vstride, col, col + nx, coef, true, dTr);
+    }
+    const double iaij = 1.0 / __ldg(a.areaT + col);
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        if (n < nt) {
+            double* __restrict__ out = a.htr[tr0 + n] + col;
+            for (int k = 0; k < nz; ++k) out[(size_t)k * ncol] = out[(size_t)k * ncol] + dTr[n][k] * iaij;
+        }
+    }
+}
+
+}  // namespace plain
+
+// ---------------------------------------------------------------------------
+// Host launchers (stream-ordered, no synchronisation).
+// ---------------------------------------------------------------------------
+cudaError_t launch_plain_phase_a(const ColumnStateArgs& cs, const SweepArgs& sw, cudaStream_t st) {
+    const int ncol = cs.nx * cs.ny;
+    launch_begin(K_COLUMN_STATE, st);
+    plain::k_column_state<<<(ncol + 127) / 128, 128, 0, st>>>(cs);
+    launch_end(K_COLUMN_STATE, st);
+    const int nface = max((sw.nx - 1) * sw.ny, sw.nx * (sw.ny - 1));
+    if (nface > 0) {
+        dim3 grid((nface + 127) / 128, 2);
+        launch_begin(K_NEUTRAL_SWEEP, st);
+        plain::k_neutral_sweep<<<grid, 128, 0, st>>>(sw);
+        launch_end(K_NEUTRAL_SWEEP, st);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_plain_phase_b(const ReconArgs& rc, const CellUpdateArgs& cu, cudaStream_t st) {
+    const int ncol = rc.nx * rc.ny;
+    // Reconstruct in groups of two tracers (register window of 2 scalars).
+    {
+        const int ngroups = (rc.ntr + 1) / 2;
+        const long long n = (long long)ncol * ngroups;
+        launch_begin(K_TRACER_RECON, st);
+        plain::k_tracer_recon<2><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc);
+        launch_end(K_TRACER_RECON, st);
+    }
+    // Update in groups of up to kCellGroup tracers.
+    for (int tr0 = 0; tr0 < cu.ntr; tr0 += kCellGroup) {
+        launch_begin(K_CELL_UPDATE, st);
+        plain::k_cell_update<kCellGroup><<<(ncol + 127) / 128, 128, 0, st>>>(cu, tr0);
+        launch_end(K_CELL_UPDATE, st);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace redi

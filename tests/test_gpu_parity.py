@@ -1,0 +1,202 @@
+"""GPU parity: the sm_100a FP64 path against the CPU oracle, through the C-ABI.
+
+The plain FP64 form is compiled with FMA contraction off and keeps the
+reference's operation order, so the bar is exact equality (0 ulp) on every
+coefficient and every tracer value, after one and after several steps. The
+reference's own tolerance for cross-implementation agreement is 1e-12 relative
+(redi/drivers/dc_main.F90:228-237); a failure message reports that figure too.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - CPU-only container
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from more_benchmarks_dc_ocean_b200 import inputs  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+REL_BAR = 1e-12
+
+
+def _rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    sc = np.maximum(np.abs(a), np.abs(b))
+    d = np.abs(a - b)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        r = np.where(sc > 1e-30, d / sc, 0.0)
+    return float(d.max(initial=0.0)), float(r.max(initial=0.0))
+
+
+def _assert_exact(name, gpu, ref):
+    gpu = np.asarray(gpu)
+    ref = np.asarray(ref)
+    assert gpu.shape == ref.shape, (name, gpu.shape, ref.shape)
+    if not np.array_equal(gpu, ref):
+        dmax, rmax = _rel(gpu, ref)
+        nbad = int(np.count_nonzero(gpu != ref))
+        pytest.fail(f"{name}: {nbad} values differ; max|diff| {dmax:.3e} max rel {rmax:.3e} (bar 0 ulp, ref bar {REL_BAR})")
+
+
+def _run_gpu(p, nsteps, redi_lib, check_coeffs=True):
+    R = redi_lib
+    dp = R.to_device(p)
+    redi = R.make_redi(dp)
+    for _ in range(nsteps):
+        assert R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms) == R.OK
+        assert R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc) == R.OK
+    torch.cuda.synchronize()
+    coeffs = {k: v.cpu().numpy() for k, v in redi.coeffs().items()} if check_coeffs else None
+    trs = [t.cpu().numpy() for t in dp.ms.tracers]
+    redi.destroy()
+    return coeffs, trs
+
+
+def _run_oracle(p, nsteps):
+    q = p.copy()
+    c = O.step(q, nsteps)
+    return c, q.tracers
+
+
+def _compare(p, nsteps, redi_lib):
+    cg, tg = _run_gpu(p, nsteps, redi_lib)
+    co, to = _run_oracle(p, nsteps)
+    for k in ("uPoL", "uPoR", "uKoL", "uKoR", "uhEff", "vPoL", "vPoR", "vKoL", "vKoR", "vhEff"):
+        _assert_exact(f"{p.name} {k}", cg[k], co[k])
+    for n, (a, b) in enumerate(zip(tg, to)):
+        _assert_exact(f"{p.name} tracer {n} after {nsteps} steps", a, b)
+
+
+def test_config0_one_step(redi_lib, oracle_lib):
+    _compare(inputs.config0(), 1, redi_lib)
+
+
+def test_config0_ten_steps(redi_lib, oracle_lib):
+    """Config 0 as BASELINE.json states it: 10 steps compared against the FP64 oracle."""
+    _compare(inputs.config0(), 10, redi_lib)
+
+
+def test_reference_ic_small(redi_lib, oracle_lib):
+    """The reference driver's own IC (dc_main.F90:172-206) at a reduced size."""
+    _compare(inputs.reference_ic(40, 30, 12), 3, redi_lib)
+
+
+@pytest.mark.parametrize("nz", [1, 2, 3, 4, 7])
+def test_short_columns(redi_lib, oracle_lib, nz):
+    """PCM ends, the nk<=2 edge cases of redi_interface_scalar and the sweep."""
+    _compare(inputs.make_problem(17, 13, nz, n_seamounts=3, land_fraction=0.2, seed=11 + nz), 2, redi_lib)
+
+
+def test_open_boundaries_and_scalar_khtr(redi_lib, oracle_lib):
+    """Non-WALL edges (flux crosses into the halo) and the scalar-khtr path (no ext arrays)."""
+    p = inputs.make_problem(24, 20, 9, seed=5)
+    p.walls = (0, 1, 0, 0)
+    R = redi_lib
+    dp = R.to_device(p)
+    redi = R.make_redi(dp)
+    redi.khtr = 1000.0
+    for _ in range(2):
+        R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms)
+        R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, None, None, dp.bc)
+    torch.cuda.synchronize()
+    tg = [t.cpu().numpy() for t in dp.ms.tracers]
+    redi.destroy()
+    co, to = _run_oracle(p, 2)  # khtr_u/v arrays hold 1000 everywhere: same per-face values
+    for n, (a, b) in enumerate(zip(tg, to)):
+        _assert_exact(f"open/scalar tracer {n}", a, b)
+
+
+def test_uniform_fields_tie_break(redi_lib, oracle_lib):
+    """Horizontally uniform T/S: dRho == 0 everywhere, the sweep's tie-break branch."""
+    p = inputs.make_problem(12, 10, 6, n_seamounts=0, land_fraction=0.0, seed=3)
+    p.h[:] = 100.0
+    zc = (np.arange(6)[::-1] + 0.5) * 100.0
+    for n, base in enumerate((10.0, 35.0)):
+        p.tracers[n][:] = (base + 0.001 * zc)[:, None, None] * 100.0
+    _compare(p, 2, redi_lib)
+
+
+def test_vanished_layers_and_land(redi_lib, oracle_lib):
+    """Zero-thickness layers (PCM next to vanished layers, H_DIV_EPS floors) and large land fraction."""
+    p = inputs.make_problem(20, 16, 8, n_seamounts=4, land_fraction=0.5, seed=21)
+    rng = np.random.default_rng(0)
+    mask = rng.random(p.h.shape) < 0.15
+    p.h[mask] = 0.0
+    for t in p.tracers:
+        t[mask] = 0.0
+    _compare(p, 2, redi_lib)
+
+
+def test_many_tracers_fused(redi_lib, oracle_lib):
+    """T, S and passive tracers in one fused apply (odd count exercises partial groups)."""
+    _compare(inputs.make_problem(30, 22, 10, n_passive=5, seed=9), 2, redi_lib)
+
+
+def test_compat_launcher_matches_oracle(redi_lib, oracle_lib):
+    """redi_opt_launch / redi_cuda_launch_ exports, called like the reference bridge."""
+    R = redi_lib
+    for symbol in ("redi_opt_launch", "redi_cuda_launch_"):
+        p = inputs.make_problem(26, 18, 11, seed=13)
+        dp = R.to_device(p)
+        nx, ny, nz, ns = p.nx, p.ny, p.nz, p.ns
+        c = {}
+        for side, (a, b) in (("u", (ny, nx + 1)), ("v", (ny + 1, nx))):
+            c[side + "PoL"] = torch.zeros((ns, a, b), dtype=torch.float64, device="cuda")
+            c[side + "PoR"] = torch.zeros((ns, a, b), dtype=torch.float64, device="cuda")
+            c[side + "KoL"] = torch.ones((ns, a, b), dtype=torch.int32, device="cuda")
+            c[side + "KoR"] = torch.ones((ns, a, b), dtype=torch.int32, device="cuda")
+            c[side + "hEff"] = torch.zeros((ns - 1, a, b), dtype=torch.float64, device="cuda")
+        ku = torch.zeros_like(dp.khtr_u_ext)
+        kv = torch.zeros_like(dp.khtr_v_ext)
+        snap = torch.zeros_like(dp.ms.tracers[0])
+        m = dp.metrics
+        R.redi_opt_launch(nx, ny, nz, p.dt, p.nghost, p.nx_phys, p.ny_phys, (1, 1, 1, 1), dp.eos, dp.ms.h_layer,
+                          dp.ms.tracers[0], dp.ms.tracers[1], m.wet_u, m.wet_v, c, dp.khtr_u_ext, dp.khtr_v_ext,
+                          ku, kv, m.dy_cu, m.dx_cv, m.idxCu, m.idyCv, m.areaT, snap, symbol=symbol)
+        co, to = _run_oracle(p, 1)
+        for k in co:
+            _assert_exact(f"{symbol} {k}", c[k].cpu().numpy(), co[k])
+        for n in range(2):
+            _assert_exact(f"{symbol} tracer {n}", dp.ms.tracers[n].cpu().numpy(), to[n])
+        assert torch.equal(ku, dp.khtr_u_ext) and torch.equal(kv, dp.khtr_v_ext)
+
+
+def test_gates_are_noops(redi_lib):
+    """The reference's early returns: disabled handle, unregistered T/S, nz mismatch, khtr<=0 without ext."""
+    R = redi_lib
+    p = inputs.make_problem(10, 8, 5, seed=2)
+    dp = R.to_device(p)
+    before = [t.clone() for t in dp.ms.tracers]
+    redi = R.OceanRedi()
+    redi.init(dp.grid, p.nz)
+    assert R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms) == R.SKIPPED  # enable = .false.
+    redi.enable = True
+    ms2 = R.MultilayerState(p.nz, dp.ms.h_layer, dp.ms.tracers, 0, 2)
+    assert R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, ms2) == R.SKIPPED
+    ms3 = R.MultilayerState(p.nz + 1, dp.ms.h_layer, dp.ms.tracers, 1, 2)
+    assert R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, ms3) == R.SKIPPED
+    assert R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, p.dt, None, None, None) == R.SKIPPED  # khtr = 0
+    torch.cuda.synchronize()
+    for a, b in zip(before, dp.ms.tracers):
+        assert torch.equal(a, b)
+    redi.destroy()
+
+
+def test_invalid_arguments_raise(redi_lib):
+    R = redi_lib
+    p = inputs.make_problem(10, 8, 5, seed=2)
+    dp = R.to_device(p)
+    redi = R.make_redi(dp)
+    bad = R.HGrid(p.nx + 1, p.ny, p.nx_phys, p.ny_phys, p.nghost)
+    with pytest.raises(R.RediError):
+        R.redi_calc_coeffs(bad, dp.metrics, dp.eos, redi, dp.ms)
+    eos = R.OceanEos(variant=1)
+    with pytest.raises(R.RediError):
+        R.redi_calc_coeffs(dp.grid, dp.metrics, eos, redi, dp.ms)
+    redi.destroy()
+    with pytest.raises(R.RediError):
+        R.OceanRedi().init(dp.grid, 4096)
