@@ -1,0 +1,466 @@
+"""Benchmark of the Redi neutral-diffusion step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--config config1|config3|config0] [--precision fp64|mixed]
+
+One step = redi_calc_coeffs + redi_apply_flux over every tracer of the domain.
+Metric: tracer-cell updates/s = N_tracers * nx_phys * ny_phys * nz
+/ t_step, land cells included; `value` sums all ranks.
+
+* value: inputs resident in HBM, K steps timed with CUDA events on the
+  launching stream between a barrier + synchronize on both sides, max over ranks.
+  Every field (0.94 GB per tracer at 1440x1080x75) exceeds the 126 MB L2, so
+  no flush is needed between steps.
+* e2e: the same metric through the public entry points with the model state
+  resident in pinned HOST memory: every step copies h and every tracer host to
+  device, runs the step and copies every tracer back.
+* roofline: the dominant kernel (most device time in the timed region, from
+  CUDA event pairs the library records around each launch on its stream);
+  achieved = algorithmic bytes per launch / mean launch time.
+* cpu_baseline: the CPU oracle (a restatement of the reference's
+  do-concurrent CPU path, OpenMP over all host cores) on a row band of the
+  same workload, rank 0 at N=1.
+* --impl reference: the reference arm — the same CPU implementation on the
+  same workload, timed per step on a bounded row band (the reference's Fortran
+  DATA=none build cannot be compiled without a Fortran compiler).
+
+For N > 1 each rank owns one 1440x1080x75 tile of an N-tile global domain
+(weak scaling); tiles exchange a halo of h and every tracer with their
+neighbours over NCCL before each step (the only data exchange the path has).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Redi tracer-cell updates/s, HBM GB/s; mixed+batched vs FP64 plain, 1 B200"
+UNIT = "tracer-cell updates/s"
+KERNEL_NAMES = ["k_column_state", "k_neutral_sweep", "k_tracer_recon", "k_cell_update", "k_mixed_recon",
+                "k_mixed_cell_update", "k_mixed_sweep", "k_domain_persistent", "aux"]
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _rank_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def _problem(name: str, grid: str | None = None):
+    from more_benchmarks_dc_ocean_b200 import inputs
+
+    if grid:
+        nxp, nyp, nz = (int(v) for v in grid.lower().split("x"))
+        return inputs.make_problem(nxp, nyp, nz, n_seamounts=40 if nxp * nyp > 200000 else 6,
+                                   land_fraction=0.30 if nxp * nyp > 200000 else 0.15, name=f"grid_{grid}")
+    return getattr(inputs, name)()
+
+
+def _sizes(p):
+    nx, ny, nz = p.nx, p.ny, p.nz
+    return dict(Nt=nx * ny * nz, ncol=nx * ny, Fu=(nx + 1) * ny, Fv=nx * (ny + 1), ns=2 * nz + 2, ntr=p.ntr)
+
+
+def boundary_bytes(p, precision: str = "fp64") -> float:
+    """Algorithmic HBM bytes of one step, boundary model: Phase A reads h, T, S and
+    writes the coefficients, Phase B reads h and the coefficients once and
+    reads + writes every tracer; plus the 2-D face/cell metrics."""
+    s = _sizes(p)
+    per_surf = 32 if precision == "fp64" else 24  # Po x2 f64, Ko x2 i32|i16, hEff f64|f32 (ns-1 ~ ns)
+    bcoef = (s["Fu"] + s["Fv"]) * s["ns"] * per_surf
+    b2d = 8 * (s["Fu"] + s["Fv"]) * 4 + 8 * s["ncol"]
+    return 8 * s["Nt"] * (3 + 1 + 2 * s["ntr"]) + 2 * bcoef + b2d
+
+
+def kernel_bytes(p, kid: int, precision: str = "fp64") -> float:
+    """Algorithmic bytes one launch of kernel `kid` must move (its share of the boundary model)."""
+    s = _sizes(p)
+    per_surf = 32 if precision == "fp64" else 24
+    bcoef = (s["Fu"] + s["Fv"]) * s["ns"] * per_surf
+    face2d = 8 * (s["Fu"] + s["Fv"]) * 4 + 8 * s["ncol"]
+    if kid == 0:   # column state: read h, T, S
+        return 24.0 * s["Nt"]
+    if kid in (1, 6):  # neutral sweep: write the coefficients
+        return float(bcoef)
+    if kid in (2, 4):  # tracer reconstruction: read h and every tracer
+        return 8.0 * s["Nt"] * (1 + s["ntr"])
+    if kid in (3, 5):  # cell update: read coefficients once, read+write every tracer
+        return float(bcoef + 16 * s["Nt"] * s["ntr"] + face2d)
+    return 0.0
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons of one GPU, sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.uuid:
+                cmd.insert(1, f"--id={self.uuid}")
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        pw = [float(r[3]) for r in rows if re.match(r"^[\d.]+$", r[3])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
+
+
+def _ncu_traffic() -> dict:
+    """Per-launch DRAM traffic (bytes) of each kernel at 1440x1080x75, from the committed ncu summaries."""
+    out = {}
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return out
+    for fn in os.listdir(d):
+        if not fn.endswith(".md"):
+            continue
+        for line in open(os.path.join(d, fn)):
+            m = re.match(r"^traffic_bytes_per_launch_full:\s*(\w+)\s*=\s*([\d.eE+]+)", line.strip())
+            if m:
+                out[m.group(1)] = float(m.group(2))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle sample (cpu_baseline and the reference arm)
+# ---------------------------------------------------------------------------
+def _row_band(p, nrows: int):
+    """Rows [0, nrows) of the physical domain (with its ghost rows) as a standalone problem."""
+    from more_benchmarks_dc_ocean_b200.inputs import RediProblem
+
+    g = p.nghost
+    ny = nrows + 2 * g
+    sl = slice(0, ny)
+    return RediProblem(
+        name=f"{p.name}_rows{nrows}", nx_phys=p.nx_phys, ny_phys=nrows, nz=p.nz, nghost=g, dt=p.dt, eos=p.eos,
+        h=np.ascontiguousarray(p.h[:, sl, :]), tracers=[np.ascontiguousarray(t[:, sl, :]) for t in p.tracers],
+        idx_temperature=p.idx_temperature, idx_salinity=p.idx_salinity,
+        dy_cu=np.ascontiguousarray(p.dy_cu[sl]), dx_cv=np.ascontiguousarray(p.dx_cv[: ny + 1]),
+        idxCu=np.ascontiguousarray(p.idxCu[sl]), idyCv=np.ascontiguousarray(p.idyCv[: ny + 1]),
+        areaT=np.ascontiguousarray(p.areaT[sl]), wet_u=np.ascontiguousarray(p.wet_u[sl]),
+        wet_v=np.concatenate([p.wet_v[:ny], np.zeros((1, p.nx))]),
+        khtr_u=np.ascontiguousarray(p.khtr_u[sl]), khtr_v=np.ascontiguousarray(p.khtr_v[: ny + 1]),
+        walls=p.walls, meta=dict(p.meta))
+
+
+def cpu_sample(p, target_s: float, nsteps: int = 1, warmup: int = 0):
+    """Time the oracle on a row band of p sized for ~target_s per step; returns (updates/s, info)."""
+    from oracle import oracle as O
+
+    threads = len(os.sched_getaffinity(0))
+    probe = _row_band(p, 2)
+    t0 = time.perf_counter()
+    O.step(probe.copy(), 1, nthreads=threads)
+    t_probe = max(time.perf_counter() - t0, 1e-3)
+    rows = int(max(1, min(p.ny_phys, math.floor(2 * target_s / t_probe))))
+    band = _row_band(p, rows)
+    times = []
+    for s in range(warmup + nsteps):
+        q = band.copy()
+        t0 = time.perf_counter()
+        O.step(q, 1, nthreads=threads)
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            times.append(dt)
+    t = min(times)
+    upd = band.ntr * band.nx_phys * band.ny_phys * band.nz / t
+    return upd, {"cores": threads, "rows": rows, "t_step_s": t, "times_s": times,
+                 "sample": f"{band.nx_phys}x{rows}x{band.nz} row band of {p.name} ({band.ntr} tracers), "
+                           f"min of {len(times)} step(s)"}
+
+
+# ---------------------------------------------------------------------------
+# Reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    p = _problem(args.config, args.grid)
+    budget = 150.0
+    per_step = max(2.0, budget / max(1, args.steps + args.warmup))
+    upd, info = cpu_sample(p, per_step, nsteps=args.steps, warmup=args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": upd, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": info["t_step_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": _config_block(p, args, world),
+        "cpu_baseline": {"value": upd, "unit": UNIT, "cores": info["cores"], "kind": "port",
+                         "sample": info["sample"]},
+        "e2e": {"value": upd, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU path (do-concurrent DATA=none restated in C++, OpenMP over all host cores); "
+                "the Fortran build itself needs a Fortran compiler, absent on this image",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _config_block(p, args, world):
+    return {
+        "workload": f"{args.grid or args.config}: {'plain FP64' if args.precision == 'fp64' else 'mixed-precision'} Redi step "
+                    f"{p.nx_phys}x{p.ny_phys}x{p.nz}, nghost {p.nghost}, {p.ntr} tracers"
+                    + (f", {world} tiles" if world > 1 else ""),
+        "grid": [p.nx_phys, p.ny_phys, p.nz], "tracers": p.ntr, "dt_s": p.dt, "khtr_m2s": float(p.khtr_u.flat[0]),
+        "land_fraction": round(p.meta.get("land_fraction", 0.0), 4), "precision": args.precision,
+        "l2": ("inputs larger than L2 (126 MB), no flush" if 8 * p.nx * p.ny * p.nz > 126e6
+               else "fields smaller than L2: not a headline configuration"),
+        "parallelism": f"dp{world}" if world > 1 else "1 GPU",
+    }
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+
+    from more_benchmarks_dc_ocean_b200 import ocean_redi as R
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    from more_benchmarks_dc_ocean_b200 import halo
+
+    p = _problem(args.config, args.grid)
+    tiling = halo.Tiling.for_world(world, rank, p) if world > 1 else None
+    if tiling is not None:
+        p = tiling.local_problem(p)
+    prec = R.FP64 if args.precision == "fp64" else R.MIXED
+    dp = R.to_device(p, dev)
+    redi = R.make_redi(dp, prec)
+    ex = None
+    if tiling is not None:
+        ex = halo.HaloExchange(tiling, dp)
+        ex.setup_masks(dp, p.wet)
+        ex.exchange()
+    st = torch.cuda.current_stream()
+    L = R.lib()
+    L.redi_b200_launch_count.restype = C.c_ulonglong
+    L.redi_b200_launch_count.argtypes = [C.c_int]
+
+    def one_step():
+        if ex is not None:
+            ex.exchange()
+        R.step(dp, redi, 1, st)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident inputs ----
+    clocks = ClockSampler(_uuid(local_rank))
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    L.redi_b200_profile_begin()
+    n0 = L.redi_b200_launch_count(-1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        one_step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    n1 = L.redi_b200_launch_count(-1)
+    ktime = (C.c_double * 9)()
+    kcount = (C.c_ulonglong * 9)()
+    L.redi_b200_profile_end(ktime, kcount, 9)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms_all = _max_over_ranks(ms, dist, dev)
+
+    upd_per_rank = p.ntr * p.nx_phys * p.ny_phys * p.nz
+    value = upd_per_rank * world / (ms_all * 1e-3)
+    kern = {KERNEL_NAMES[k]: {"ms_total": ktime[k], "launches": int(kcount[k]),
+                              "ms_per_launch": ktime[k] / kcount[k]} for k in range(9) if kcount[k]}
+    top = max((k for k in range(9) if kcount[k]), key=lambda k: ktime[k])
+    peak, peak_kind = _peaks()
+    bytes_launch = kernel_bytes(p, top, args.precision)
+    t_launch = ktime[top] / kcount[top] * 1e-3
+    achieved = bytes_launch / t_launch / 1e9
+    traffic = _ncu_traffic().get(KERNEL_NAMES[top]) if (p.nx_phys, p.ny_phys, p.nz) == (1440, 1080, 75) else None
+    bstep = boundary_bytes(p, args.precision)
+
+    # ---- e2e: host-resident state through the public entry points ----
+    e2e = None
+    if not args.no_e2e:
+        e2e = _e2e(args, p, dp, redi, ex, st, dist, dev, world)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        upd, info = cpu_sample(p, args.cpu_seconds)
+        cpu = {"value": upd, "unit": UNIT, "cores": info["cores"], "kind": "port", "sample": info["sample"]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_all, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32", "data": "synthetic",
+            "config": _config_block(p, args, world),
+            "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[top], "achieved": achieved, "peak": peak,
+                         "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": bytes_launch},
+            "step_roofline": {"boundary_bytes_per_step": bstep, "achieved_gbs": bstep / (ms_all * 1e-3) / 1e9,
+                              "frac": bstep / (ms_all * 1e-3) / 1e9 / peak},
+            "kernels": kern,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk,
+            "gpu_launches": int(n1 - n0),
+            "hbm_gbs_per_rank": bstep / (ms_all * 1e-3) / 1e9,
+        }
+        print(json.dumps(line), flush=True)
+    redi.destroy()
+    if ex is not None:
+        ex.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _uuid(local_rank):
+    try:
+        import torch
+
+        u = str(torch.cuda.get_device_properties(local_rank).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
+
+
+def _max_over_ranks(x, dist, dev):
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _e2e(args, p, dp, redi, ex, st, dist, dev, world):
+    import torch
+
+    from more_benchmarks_dc_ocean_b200 import ocean_redi as R
+
+    host_h = torch.from_numpy(np.ascontiguousarray(p.h)).pin_memory()
+    host_tr = [torch.from_numpy(np.ascontiguousarray(t)).pin_memory() for t in p.tracers]
+
+    def e2e_step():
+        dp.ms.h_layer.copy_(host_h, non_blocking=True)
+        for d, h in zip(dp.ms.tracers, host_tr):
+            d.copy_(h, non_blocking=True)
+        if ex is not None:
+            ex.exchange()
+        R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, st)
+        R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, st)
+        for d, h in zip(dp.ms.tracers, host_tr):
+            h.copy_(d, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
+    nt = p.nx * p.ny * p.nz
+    return {"value": p.ntr * p.nx_phys * p.ny_phys * p.nz * world / (ms * 1e-3), "unit": UNIT,
+            "h2d_bytes_per_step": 8 * nt * (1 + p.ntr), "d2h_bytes_per_step": 8 * nt * p.ntr, "ms_per_step": ms,
+            "host_memory": "pinned"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="config1", choices=["config0", "config1", "config3"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--grid", default=None, help="NXxNYxNZ: a generated domain of that size instead of --config")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    rank, world, local_rank = _rank_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_b200(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -96,6 +96,7 @@ class RediProblem:
     khtr_v: np.ndarray         # (ny+1, nx)
     walls: tuple = (1, 1, 1, 1)  # west, east, south, north: 1 = no-normal-flow wall
     meta: dict = field(default_factory=dict)
+    wet: Optional[np.ndarray] = None  # (ny, nx) cell wet flag (1 = ocean), where known
 
     @property
     def nx(self) -> int:
@@ -240,6 +241,7 @@ def make_problem(nx_phys: int, ny_phys: int, nz: int, *, n_seamounts: int = 6, l
         areaT=np.full((ny, nx), dx * dx),
         wet_u=wet_u, wet_v=wet_v,
         khtr_u=np.full((ny, nx + 1), khtr), khtr_v=np.full((ny + 1, nx), khtr),
+        wet=wet.astype(np.float64),
         meta={"seed": seed, "n_seamounts": n_seamounts, "land_fraction_target": land_fraction,
               "land_fraction": float(1.0 - wet[nghost:nghost + ny_phys, nghost:nghost + nx_phys].mean()),
               "seamount_scale": scale, "n_passive": n_passive},
@@ -307,5 +309,5 @@ def reference_ic(nx_phys: int = 473, ny_phys: int = 297, nz: int = 30) -> RediPr
         areaT=np.full((ny, nx), 8000.0 * 11100.0),
         wet_u=np.ones((ny, nx + 1)), wet_v=np.ones((ny + 1, nx)),
         khtr_u=np.full((ny, nx + 1), 100.0), khtr_v=np.full((ny + 1, nx), 100.0),
-        meta={"source": "redi/drivers/dc_main.F90:172-206"},
+        wet=np.ones((ny, nx)), meta={"source": "redi/drivers/dc_main.F90:172-206"},
     )
