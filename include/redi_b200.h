@@ -144,6 +144,12 @@ REDI_B200_API int redi_b200_get_coeffs(const redi_b200* self, redi_b200_coeffs* 
 /* Bytes of device scratch the handle holds beside its coefficient slots. */
 REDI_B200_API long long redi_b200_workspace_bytes(const redi_b200* self);
 
+/* Number of coefficient sublayers the cell update found out of order (cell-side
+ * Ko decreasing along a face, or outside 1..nz) since the last reset; always 0
+ * for coefficients produced by redi_b200_calc_coeffs. Synchronises the device.
+ * reset != 0 zeroes the count. (No counterpart in the reference.) */
+REDI_B200_API int redi_b200_error_count(const redi_b200* self, int reset);
+
 /* Message of the last error on the calling thread ("" if none). */
 REDI_B200_API const char* redi_b200_last_error(void);
 

@@ -52,14 +52,20 @@ cudaError_t fill_int(int* p, size_t n, int v, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// Grow-only device scratch.
+// Grow-only device scratch. The first 256 bytes hold the device error word
+// (count of out-of-order coefficient sublayers seen by the cell update); phase
+// data starts at data().
 struct Scratch {
+    static constexpr size_t kHeader = 256;
     void* ptr = nullptr;
     size_t bytes = 0;
     int device = -1;
     cudaError_t reserve(size_t need) {
+        need += kHeader;
         if (need <= bytes) return cudaSuccess;
+        int err_keep = 0;
         if (ptr) {
+            cudaMemcpy(&err_keep, ptr, sizeof(int), cudaMemcpyDeviceToHost);
             cudaError_t e = cudaFree(ptr);
             ptr = nullptr;
             bytes = 0;
@@ -71,8 +77,10 @@ struct Scratch {
             return e;
         }
         bytes = need;
-        return cudaSuccess;
+        return cudaMemcpy(ptr, &err_keep, sizeof(int), cudaMemcpyHostToDevice);
     }
+    void* data() const { return static_cast<char*>(ptr) + kHeader; }
+    int* err() const { return static_cast<int*>(ptr); }
     void release() {
         if (ptr) cudaFree(ptr);
         ptr = nullptr;
@@ -103,7 +111,7 @@ int run_plain_phase_a(int nx, int ny, int nz, const redi::EosLin& eos, const dou
     redi::ColumnStateArgs cs{};
     cs.nx = nx; cs.ny = ny; cs.nz = nz; cs.eos = eos;
     cs.h = h; cs.th = th; cs.sh = sh;
-    cs.ifc = reinterpret_cast<redi::IfcState*>(ws.ptr);
+    cs.ifc = reinterpret_cast<redi::IfcState*>(ws.data());
     cs.pint = reinterpret_cast<double*>(cs.ifc + nifc);
     redi::SweepArgs sw{};
     sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos.rho0;
@@ -131,7 +139,7 @@ int run_plain_phase_b(const PhaseBInputs& in, int ntr, double* const* htr, Scrat
         const int nt = (ntr - t0) < group ? (ntr - t0) : group;
         redi::ReconArgs rc{};
         rc.nx = in.nx; rc.ny = in.ny; rc.nz = in.nz; rc.ntr = nt; rc.h = in.h;
-        rc.ti = reinterpret_cast<double*>(ws.ptr);
+        rc.ti = reinterpret_cast<double*>(ws.data());
         rc.ppm = reinterpret_cast<redi::PpmLayer*>(rc.ti + (size_t)nt * ncol * (in.nz + 1));
         redi::CellUpdateArgs cu{};
         cu.nx = in.nx; cu.ny = in.ny; cu.nz = in.nz; cu.ntr = nt;
@@ -139,7 +147,7 @@ int run_plain_phase_b(const PhaseBInputs& in, int ntr, double* const* htr, Scrat
         cu.wall_w = in.walls[0]; cu.wall_e = in.walls[1]; cu.wall_s = in.walls[2]; cu.wall_n = in.walls[3];
         cu.dt = in.dt; cu.khtr = in.khtr; cu.khtr_u = in.khtr_u; cu.khtr_v = in.khtr_v;
         cu.dy_cu = in.dy_cu; cu.dx_cv = in.dx_cv; cu.idxCu = in.idxCu; cu.idyCv = in.idyCv; cu.areaT = in.areaT;
-        cu.u = in.u; cu.v = in.v; cu.ti = rc.ti; cu.ppm = rc.ppm;
+        cu.u = in.u; cu.v = in.v; cu.ti = rc.ti; cu.ppm = rc.ppm; cu.err = ws.err();
         for (int n = 0; n < nt; ++n) {
             rc.htr[n] = htr[t0 + n];
             cu.htr[n] = htr[t0 + n];
@@ -358,6 +366,16 @@ int redi_b200_get_coeffs(const redi_b200* s, redi_b200_coeffs* out) {
 }
 
 long long redi_b200_workspace_bytes(const redi_b200* s) { return s ? (long long)s->ws.bytes : 0; }
+
+int redi_b200_error_count(const redi_b200* s, int reset) {
+    if (!s) return fail(REDI_B200_E_ARG, "redi_b200_error_count: handle is NULL");
+    if (!s->ws.ptr) return 0;
+    int v = 0;
+    cudaError_t e = cudaMemcpy(&v, s->ws.err(), sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "redi_b200_error_count");
+    if (reset) cudaMemset(s->ws.err(), 0, sizeof(int));
+    return v;
+}
 
 int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
                           redi_b200* s, const redi_b200_state* ms, void* stream) {

@@ -33,8 +33,8 @@ struct ColumnStateArgs {
     const double* h;
     const double* th;
     const double* sh;
-    IfcState* ifc;   // [column][nz+1]
-    double* pint;    // [column][nz+1]
+    IfcState* ifc;   // [nz+1][column]
+    double* pint;    // [nz+1][column]
 };
 
 struct SweepArgs {
@@ -51,8 +51,8 @@ struct ReconArgs {
     int nx, ny, nz, ntr;
     const double* h;
     const double* htr[kMaxTracers];
-    double* ti;      // [tracer][column][nz+1]
-    PpmLayer* ppm;   // [tracer][column][nz]
+    double* ti;      // [tracer][nz+1][column]
+    PpmLayer* ppm;   // [tracer][nz][column]
 };
 
 struct CellUpdateArgs {
@@ -69,9 +69,10 @@ struct CellUpdateArgs {
     const double* idyCv;
     const double* areaT;
     FaceIn u, v;
-    const double* ti;
-    const PpmLayer* ppm;
+    const double* ti;       // [tracer][nz+1][column]
+    const PpmLayer* ppm;    // [tracer][nz][column]
     double* htr[kMaxTracers];
+    int* err;               // device error word (sublayers out of order), may be null
 };
 
 // Scratch bytes each phase needs for an (nx, ny, nz) domain with ntr tracers.

@@ -108,7 +108,7 @@ __device__ __forceinline__ void stream_edges(int nk, Load load, Emit emit) {
 
 // ---------------------------------------------------------------------------
 // Phase A, step 1: per-column interface state (redi_build_column,
-// ocean_redi.F90:609-654).
+// ocean_redi.F90:609-654), written in [interface][column] order.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a) {
     const int ncol = a.nx * a.ny;
@@ -118,8 +118,8 @@ __global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a) {
     const double* __restrict__ h = a.h + col;
     const double* __restrict__ th = a.th + col;
     const double* __restrict__ sh = a.sh + col;
-    IfcState* __restrict__ ifc = a.ifc + (size_t)col * (nz + 1);
-    double* __restrict__ pint = a.pint + (size_t)col * (nz + 1);
+    IfcState* __restrict__ ifc = a.ifc + col;
+    double* __restrict__ pint = a.pint + col;
 
     const EosLin eos = a.eos;
     const double dsv_dt = eos.alpha_T / (eos.rho0 * eos.rho0);  // ocean_eos.F90:511
@@ -139,15 +139,10 @@ __global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a) {
     auto emit = [&](int t, const double (&e)[2], const double (&)[2]) {
         if (t >= 2) P = P + grho * h_layer_above;  // Pint(t) = Pint(t-1) + g*rho0*h(t-1)
         const double rho_i = eos.rho0 + eos.beta_S * (e[1] - eos.S_ref) - eos.alpha_T * (e[0] - eos.T_ref);
-        IfcState s;
-        s.T = e[0];
-        s.S = e[1];
-        s.dRdT = -(rho_i * rho_i) * dsv_dt;
-        s.dRdS = -(rho_i * rho_i) * dsv_ds;
-        double2* q = reinterpret_cast<double2*>(ifc + (t - 1));
-        q[0] = make_double2(s.T, s.S);
-        q[1] = make_double2(s.dRdT, s.dRdS);
-        pint[t - 1] = P;
+        double2* q = reinterpret_cast<double2*>(ifc + (size_t)(t - 1) * ncol);
+        q[0] = make_double2(e[0], e[1]);
+        q[1] = make_double2(-(rho_i * rho_i) * dsv_dt, -(rho_i * rho_i) * dsv_ds);
+        pint[(size_t)(t - 1) * ncol] = P;
         if (t <= nz) h_layer_above = __ldg(h + (size_t)(nz - t) * ncol);
     };
     stream_edges<2>(nz, load, emit);
@@ -157,10 +152,62 @@ __global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a) {
 // Phase A, step 2: the continuous neutral-surface sweep per face
 // (redi_neutral_positions_continuous + redi_face_coeffs, ocean_redi.F90:307-464,
 // 656-692) and the slot writes of redi_calc_coeffs_x/_y (:694-812).
+//
+// Each column is read through a three-interface register window anchored at
+// km1 = max(k-1, 1) (the reference's klm1/krm1): interfaces km1, km1+1 and
+// km1+2 with their pressures. The pointer's own interface is km1 (k = 1) or
+// km1+1 (k >= 2). When a pointer advances the window slides by one and one
+// interface is fetched ahead, so a step waits on no load it has just issued.
+// The two search directions share one code path: the searched column S and
+// the anchor column A are selected per step (with the reference's asymmetric
+// `dRhoTop > 0` / `dRhoTop >= 0` tests kept).
 // ---------------------------------------------------------------------------
+struct ColWin {
+    IfcState a, b, c;   // interfaces km1, km1+1, km1+2 (1-based)
+    double pa, pb, pc;  // pressures at the same interfaces
+    int k;              // the pointer (1-based, 1..nk+1)
+};
+
+__device__ __forceinline__ void win_init(ColWin& w, const IfcState* X, const double* P, int nk, size_t ld) {
+    w.k = 1;
+    const int i1 = min(1, nk), i2 = min(2, nk);
+    w.a = load_ifc(X);
+    w.b = load_ifc(X + (size_t)i1 * ld);
+    w.c = load_ifc(X + (size_t)i2 * ld);
+    w.pa = __ldg(P);
+    w.pb = __ldg(P + (size_t)i1 * ld);
+    w.pc = __ldg(P + (size_t)i2 * ld);
+}
+
+// k -> k+1: the anchor km1 moves only when k was >= 2.
+__device__ __forceinline__ void win_advance(ColWin& w, const IfcState* X, const double* P, int nk, size_t ld) {
+    if (w.k >= 2) {
+        w.a = w.b;
+        w.b = w.c;
+        w.pa = w.pb;
+        w.pb = w.pc;
+        const int inext = min(w.k + 1, nk);  // 0-based index of interface km1_new + 2
+        w.c = load_ifc(X + (size_t)inext * ld);
+        w.pc = __ldg(P + (size_t)inext * ld);
+    }
+    w.k += 1;
+}
+
+__device__ __forceinline__ IfcState sel(bool c, const IfcState& x, const IfcState& y) {
+    IfcState r;
+    r.T = c ? x.T : y.T;
+    r.S = c ? x.S : y.S;
+    r.dRdT = c ? x.dRdT : y.dRdT;
+    r.dRdS = c ? x.dRdS : y.dRdS;
+    return r;
+}
+
+__device__ __forceinline__ IfcState win_own(const ColWin& w) { return sel(w.k == 1, w.a, w.b); }
+
 __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
     const int dir = blockIdx.y;  // 0: u-faces, 1: v-faces
     const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    const size_t ld = (size_t)nx * ny;  // interface stride of the scratch
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     int colL, colR, fo, nface;
     size_t fstride;
@@ -200,25 +247,24 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
         return;
     }
 
-    const IfcState* __restrict__ L = a.ifc + (size_t)colL * (nz + 1);
-    const IfcState* __restrict__ R = a.ifc + (size_t)colR * (nz + 1);
-    const double* __restrict__ Pl = a.pint + (size_t)colL * (nz + 1);
-    const double* __restrict__ Pr = a.pint + (size_t)colR * (nz + 1);
+    const IfcState* XL = a.ifc + colL;
+    const IfcState* XR = a.ifc + colR;
+    const double* PL = a.pint + colL;
+    const double* PR = a.pint + colR;
     const double pa_to_h = 1.0 / (kGravity * a.rho0);
     const int nk = nz;
 
-    int kr = 1, kl = 1;
-    double lastP_right = 0.0, lastP_left = 0.0;
-    int lastK_right = 1, lastK_left = 1;
+    ColWin wl, wr;
+    win_init(wl, XL, PL, nk, ld);
+    win_init(wr, XR, PR, nk, ld);
+    double lastP_left = 0.0, lastP_right = 0.0;
+    int lastK_left = 1, lastK_right = 1;
     bool reached_bottom = false, search_left = false, search_right = false;
     double absL_prev = 0.0, absR_prev = 0.0;
 
     for (int ks = 1; ks <= ns; ++ks) {
-        int klm1 = max(kl - 1, 1);
-        int krm1 = max(kr - 1, 1);
-        const IfcState Lk = load_ifc(L + (kl - 1));
-        const IfcState Rk = load_ifc(R + (kr - 1));
-        const double dRho = secant_drho(Rk, Lk);
+        const int kl = wl.k, kr = wr.k;
+        const double dRho = secant_drho(win_own(wr), win_own(wl));
         if (!reached_bottom) {
             if (dRho < 0.0) {
                 search_left = true;
@@ -234,49 +280,66 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
                 search_right = !search_right;
             }
         }
-        double pol, por;
-        int kol, kor;
-        if (search_left) {
-            const IfcState La = load_ifc(L + (klm1 - 1)), Lb = load_ifc(L + klm1);
-            const double dRhoTop = secant_drho(La, Rk);
-            const double dRhoBot = secant_drho(Lb, Rk);
-            if (dRhoTop > 0.0 || kr + kl == 2) pol = 0.0;
-            else if (dRhoTop >= dRhoBot) pol = 1.0;
-            else pol = interpolate_position(dRhoTop, __ldg(Pl + klm1 - 1), dRhoBot, __ldg(Pl + klm1));
-            if (pol >= 1.0 && klm1 < nk) {
-                klm1 += 1;
-                pol = pol - 1.0;
-            }
-            if ((double)(klm1 - lastK_left) + (pol - lastP_left) < 0.0) {
-                pol = lastP_left;
-                klm1 = lastK_left;
-            }
-            kol = klm1;
-            if (kr <= nk) { por = 0.0; kor = kr; }
-            else          { por = 1.0; kor = nk; }
-            if (kr <= nk) kr += 1;
-            else { reached_bottom = true; search_right = true; search_left = false; }
-        } else {  // search_right (exactly one direction is always set)
-            const IfcState Ra = load_ifc(R + (krm1 - 1)), Rb = load_ifc(R + krm1);
-            const double dRhoTop = secant_drho(Ra, Lk);
-            const double dRhoBot = secant_drho(Rb, Lk);
-            if (dRhoTop >= 0.0 || kr + kl == 2) por = 0.0;
-            else if (dRhoTop >= dRhoBot) por = 1.0;
-            else por = interpolate_position(dRhoTop, __ldg(Pr + krm1 - 1), dRhoBot, __ldg(Pr + krm1));
-            if (por >= 1.0 && krm1 < nk) {
-                krm1 += 1;
-                por = por - 1.0;
-            }
-            if ((double)(krm1 - lastK_right) + (por - lastP_right) < 0.0) {
-                por = lastP_right;
-                krm1 = lastK_right;
-            }
-            kor = krm1;
-            if (kl <= nk) { pol = 0.0; kol = kl; }
-            else          { pol = 1.0; kol = nk; }
-            if (kl <= nk) kl += 1;
-            else { reached_bottom = true; search_right = false; search_left = true; }
+        // Exactly one direction is set. S: searched column, A: anchor column
+        // (selected field by field so both windows stay in registers).
+        const bool L = search_left;
+        const IfcState Sa = sel(L, wl.a, wr.a), Sb = sel(L, wl.b, wr.b);
+        const double Spa = L ? wl.pa : wr.pa, Spb = L ? wl.pb : wr.pb, Spc = L ? wl.pc : wr.pc;
+        const int Sk = L ? kl : kr;
+        const IfcState anc = L ? (kr == 1 ? wr.a : wr.b) : (kl == 1 ? wl.a : wl.b);
+        const double Apa = L ? wr.pa : wl.pa, Apb = L ? wr.pb : wl.pb, Apc = L ? wr.pc : wl.pc;
+        const int ka = L ? kr : kl;
+        const double dRhoTop = secant_drho(Sa, anc);
+        const double dRhoBot = secant_drho(Sb, anc);
+        const int km1 = Sk - 1 > 1 ? Sk - 1 : 1;
+        double po_s;
+        const bool top_zero = (L ? (dRhoTop > 0.0) : (dRhoTop >= 0.0)) || kr + kl == 2;
+        if (top_zero) po_s = 0.0;
+        else if (dRhoTop >= dRhoBot) po_s = 1.0;
+        else po_s = interpolate_position(dRhoTop, Spa, dRhoBot, Spb);
+        int ko_s = km1;
+        bool carried = false;
+        if (po_s >= 1.0 && km1 < nk) {
+            ko_s = km1 + 1;
+            po_s = po_s - 1.0;
+            carried = true;
         }
+        const int lastK_s = L ? lastK_left : lastK_right;
+        const double lastP_s = L ? lastP_left : lastP_right;
+        bool backstop = false;
+        if ((double)(ko_s - lastK_s) + (po_s - lastP_s) < 0.0) {
+            po_s = lastP_s;
+            ko_s = lastK_s;
+            backstop = true;
+        }
+        // absolute position of the searched side (redi_absolute_position)
+        double abs_s;
+        if (backstop) abs_s = L ? absL_prev : absR_prev;
+        else if (carried) abs_s = Spb + po_s * (Spc - Spb);
+        else abs_s = Spa + po_s * (Spb - Spa);
+        // anchor side: its own interface, or the bed once exhausted
+        double po_a, abs_a;
+        int ko_a;
+        if (ka <= nk) {
+            po_a = 0.0;
+            ko_a = ka;
+            abs_a = (ka == 1) ? Apa + po_a * (Apb - Apa) : Apb + po_a * (Apc - Apb);
+        } else {
+            po_a = 1.0;
+            ko_a = nk;
+            abs_a = Apa + po_a * (Apb - Apa);  // km1 = nk: interfaces nk, nk+1
+        }
+        if (ka <= nk) {
+            if (L) win_advance(wr, XR, PR, nk, ld);
+            else   win_advance(wl, XL, PL, nk, ld);
+        } else {
+            reached_bottom = true;
+            search_left = !L;
+            search_right = L;
+        }
+        const double pol = L ? po_s : po_a, por = L ? po_a : po_s;
+        const int kol = L ? ko_s : ko_a, kor = L ? ko_a : ko_s;
+        const double absL = L ? abs_s : abs_a, absR = L ? abs_a : abs_s;
         lastK_left = kol;
         lastP_left = pol;
         lastK_right = kor;
@@ -286,13 +349,7 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
         PoR[so] = por;
         KoL[so] = kol;
         KoR[so] = kor;
-        // redi_absolute_position (ocean_redi.F90:289-298) and the harmonic-mean
-        // effective thickness (:452-462), then Pa -> m (:688-691).
-        const double pl0 = __ldg(Pl + kol - 1), pl1 = __ldg(Pl + kol);
-        const double pr0 = __ldg(Pr + kor - 1), pr1 = __ldg(Pr + kor);
-        const double absL = pl0 + pol * (pl1 - pl0);
-        const double absR = pr0 + por * (pr1 - pr0);
-        if (ks > 1) {
+        if (ks > 1) {  // harmonic-mean effective thickness (:452-462), Pa -> m (:688-691)
             const double hL = absL - absL_prev;
             const double hR = absR - absR_prev;
             double he = 0.0;
@@ -306,8 +363,9 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
 
 // ---------------------------------------------------------------------------
 // Phase B, step 1: per-column tracer reconstruction for a group of NT tracers
-// (redi_tracer_column, ocean_redi.F90:852-891). Writes, per tracer and
-// column, the nz+1 interface values Tint and the nz prepared PPM layers.
+// (redi_tracer_column, ocean_redi.F90:852-891). Writes, per tracer, the nz+1
+// interface values Tint and the nz prepared PPM layers in [layer][column]
+// order, so that threads of neighbouring columns touch neighbouring addresses.
 // ---------------------------------------------------------------------------
 template <int NT>
 __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
@@ -328,8 +386,8 @@ __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
     for (int n = 0; n < NT; ++n) {
         const int tr = tr0 + (n < nt ? n : 0);
         htr[n] = a.htr[tr] + col;
-        ti[n] = a.ti + (size_t)tr * ncol * (nz + 1) + (size_t)col * (nz + 1);
-        ppm[n] = a.ppm + (size_t)tr * ncol * nz + (size_t)col * nz;
+        ti[n] = a.ti + (size_t)tr * ncol * (nz + 1) + col;
+        ppm[n] = a.ppm + (size_t)tr * ncol * nz + col;
     }
     double e_prev[NT];
 
@@ -345,13 +403,13 @@ __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
 #pragma unroll
         for (int n = 0; n < NT; ++n) {
             if (n < nt) {
-                ti[n][t - 1] = e[n];
+                ti[n][(size_t)(t - 1) * ncol] = e[n];
                 if (t >= 2) {  // layer t-1 is complete: limit its edges
                     double alk = e_prev[n], ark = e[n];
                     const double tlk = s_above[n];
                     ppm_limit(alk, ark, tlk);
                     const PpmLayer q = make_ppm_layer(alk, ark, tlk);
-                    double2* p = reinterpret_cast<double2*>(ppm[n] + (t - 2));
+                    double2* p = reinterpret_cast<double2*>(ppm[n] + (size_t)(t - 2) * ncol);
                     p[0] = make_double2(q.aL, q.dA);
                     p[1] = make_double2(q.a6o3, q.B);
                 }
@@ -365,81 +423,92 @@ __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
 // ---------------------------------------------------------------------------
 // Phase B, step 2: per-cell flux divergence (redi_apply_flux_impl +
 // redi_face_flux + redi_sublayer_dT, ocean_redi.F90:893-925, 1037-1181).
+//
+// One thread per T-cell column. The faces are visited in the reference order
+// W, E, S, N and, within a face, the sublayers ks = 1..ns-1 in order; all lanes
+// of a warp walk the same ks together, so the coefficient loads of a warp are
+// one contiguous row per array. Each contribution is added to the cell's dTr
+// entry for its native layer exactly as the reference adds it. The running
+// value of the current entry is held in a register while consecutive
+// sublayers hit the same layer (the cell-side Ko of a face is non-decreasing
+// in ks), and written back to the per-thread dTr array when the layer
+// changes: the same sequence of additions, with fewer local-memory accesses.
 // ---------------------------------------------------------------------------
-struct SurfInterp {  // tracer values at one neutral surface, both columns
-    double tl, tr;
-};
+__device__ __forceinline__ double interp(double P, double a, double b) { return (1.0 - P) * a + P * b; }
 
 template <int NT>
-__device__ __forceinline__ void face_accumulate(const CellUpdateArgs& a, int nt, int tr0, const FaceIn& F,
-                                                size_t fo, size_t fstride, int colL, int colR, double coef,
-                                                bool is_left, double (&dTr)[NT][kNzMax]) {
+__device__ __forceinline__ void face_accumulate(const CellUpdateArgs& a, int nt, const double* const (&ti)[NT],
+                                                const PpmLayer* const (&pp)[NT], const FaceIn& F, size_t fo,
+                                                size_t fstride, int colL, int colR, double coef, bool is_left,
+                                                double (&dTr)[NT][kNzMax]) {
     const int nz = a.nz, ns = 2 * nz + 2;
-    const int ncol = a.nx * a.ny;
-    const double* tiL[NT];
-    const double* tiR[NT];
-    const PpmLayer* pL[NT];
-    const PpmLayer* pR[NT];
-#pragma unroll
-    for (int n = 0; n < NT; ++n) {
-        const int tr = tr0 + (n < nt ? n : 0);
-        tiL[n] = a.ti + (size_t)tr * ncol * (nz + 1) + (size_t)colL * (nz + 1);
-        tiR[n] = a.ti + (size_t)tr * ncol * (nz + 1) + (size_t)colR * (nz + 1);
-        pL[n] = a.ppm + (size_t)tr * ncol * nz + (size_t)colL * nz;
-        pR[n] = a.ppm + (size_t)tr * ncol * nz + (size_t)colR * nz;
-    }
+    const size_t ncol = (size_t)a.nx * a.ny;
     const double* __restrict__ hEff = F.hEff + fo;
     const double* __restrict__ PoL = F.PoL + fo;
     const double* __restrict__ PoR = F.PoR + fo;
     const int* __restrict__ KoL = F.KoL + fo;
     const int* __restrict__ KoR = F.KoR + fo;
 
-    int cached = -1;  // surface whose interpolated tracer values are held in `top`
-    int kl_top = 1, kr_top = 1;
-    double pl_top = 0.0, pr_top = 0.0;
-    SurfInterp top[NT];
+    int cached = -1;  // surface whose tracer values are held in tl/tr
+    int kl_t = 1, kr_t = 1;
+    double pl_t = 0.0, pr_t = 0.0;
+    double tl[NT], tr[NT];
+    int cur = -1;     // dTr entry held in acc
+    double acc[NT];
 
     for (int s = 0; s < ns - 1; ++s) {
         const double he = __ldg(hEff + s * fstride);
         if (he == 0.0) continue;
         if (cached != s) {
-            kl_top = min(max(__ldg(KoL + s * fstride), 1), nz);
-            kr_top = min(max(__ldg(KoR + s * fstride), 1), nz);
-            pl_top = __ldg(PoL + s * fstride);
-            pr_top = __ldg(PoR + s * fstride);
+            kl_t = min(max(__ldg(KoL + s * fstride), 1), nz);
+            kr_t = min(max(__ldg(KoR + s * fstride), 1), nz);
+            pl_t = __ldg(PoL + s * fstride);
+            pr_t = __ldg(PoR + s * fstride);
 #pragma unroll
             for (int n = 0; n < NT; ++n) {
-                top[n].tl = (1.0 - pl_top) * __ldg(tiL[n] + kl_top - 1) + pl_top * __ldg(tiL[n] + kl_top);
-                top[n].tr = (1.0 - pr_top) * __ldg(tiR[n] + kr_top - 1) + pr_top * __ldg(tiR[n] + kr_top);
+                tl[n] = interp(pl_t, __ldg(ti[n] + (size_t)(kl_t - 1) * ncol + colL), __ldg(ti[n] + (size_t)kl_t * ncol + colL));
+                tr[n] = interp(pr_t, __ldg(ti[n] + (size_t)(kr_t - 1) * ncol + colR), __ldg(ti[n] + (size_t)kr_t * ncol + colR));
             }
         }
-        const int kl_bot = min(max(__ldg(KoL + (s + 1) * fstride), 1), nz);
-        const int kr_bot = min(max(__ldg(KoR + (s + 1) * fstride), 1), nz);
-        const double pl_bot = __ldg(PoL + (s + 1) * fstride);
-        const double pr_bot = __ldg(PoR + (s + 1) * fstride);
-        const double xRl = pl_bot + (double)(kl_bot - kl_top);
-        const double xRr = pr_bot + (double)(kr_bot - kr_top);
-        const int knat = is_left ? nz - kl_top : nz - kr_top;
-        SurfInterp bot[NT];
+        const size_t s1 = (size_t)(s + 1) * fstride;
+        const int kl_b = min(max(__ldg(KoL + s1), 1), nz);
+        const int kr_b = min(max(__ldg(KoR + s1), 1), nz);
+        const double pl_b = __ldg(PoL + s1);
+        const double pr_b = __ldg(PoR + s1);
+        const double xRl = pl_b + (double)(kl_b - kl_t);
+        const double xRr = pr_b + (double)(kr_b - kr_t);
+        const int knat = is_left ? nz - kl_t : nz - kr_t;
+        if (knat != cur) {
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                if (cur >= 0) dTr[n][cur] = acc[n];
+                acc[n] = dTr[n][knat];
+            }
+            cur = knat;
+        }
 #pragma unroll
         for (int n = 0; n < NT; ++n) {
-            bot[n].tl = (1.0 - pl_bot) * __ldg(tiL[n] + kl_bot - 1) + pl_bot * __ldg(tiL[n] + kl_bot);
-            bot[n].tr = (1.0 - pr_bot) * __ldg(tiR[n] + kr_bot - 1) + pr_bot * __ldg(tiR[n] + kr_bot);
+            const double bl = interp(pl_b, __ldg(ti[n] + (size_t)(kl_b - 1) * ncol + colL), __ldg(ti[n] + (size_t)kl_b * ncol + colL));
+            const double br = interp(pr_b, __ldg(ti[n] + (size_t)(kr_b - 1) * ncol + colR), __ldg(ti[n] + (size_t)kr_b * ncol + colR));
             if (n < nt) {
-                const double tlay = ppm_ave(pl_top, xRl, load_ppm(pL[n] + kl_top - 1));
-                const double trlay = ppm_ave(pr_top, xRr, load_ppm(pR[n] + kr_top - 1));
-                const double dT = guarded_dT(top[n].tr - top[n].tl, bot[n].tr - bot[n].tl, trlay - tlay);
+                const double tlay = ppm_ave(pl_t, xRl, load_ppm(pp[n] + (size_t)(kl_t - 1) * ncol + colL));
+                const double trlay = ppm_ave(pr_t, xRr, load_ppm(pp[n] + (size_t)(kr_t - 1) * ncol + colR));
+                const double dT = guarded_dT(tr[n] - tl[n], br - bl, trlay - tlay);
                 const double flx = dT * he * coef;
-                if (is_left) dTr[n][knat] = dTr[n][knat] + flx;
-                else         dTr[n][knat] = dTr[n][knat] - flx;
+                acc[n] = is_left ? acc[n] + flx : acc[n] - flx;
             }
-            top[n] = bot[n];
+            tl[n] = bl;
+            tr[n] = br;
         }
         cached = s + 1;
-        kl_top = kl_bot;
-        kr_top = kr_bot;
-        pl_top = pl_bot;
-        pr_top = pr_bot;
+        kl_t = kl_b;
+        kr_t = kr_b;
+        pl_t = pl_b;
+        pr_t = pr_b;
+    }
+    if (cur >= 0) {
+#pragma unroll
+        for (int n = 0; n < NT; ++n) dTr[n][cur] = acc[n];
     }
 }
 
@@ -455,6 +524,14 @@ __global__ void __launch_bounds__(128) k_cell_update(CellUpdateArgs a, int tr0) 
     const int wuf_w = a.nghost + 1, wuf_e = a.nghost + a.nxp + 1;
     const int wvf_s = a.nghost + 1, wvf_n = a.nghost + a.nyp + 1;
 
+    const double* ti[NT];
+    const PpmLayer* pp[NT];
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        const int tr = tr0 + (n < nt ? n : 0);
+        ti[n] = a.ti + (size_t)tr * ncol * (nz + 1);
+        pp[n] = a.ppm + (size_t)tr * ncol * nz;
+    }
     double dTr[NT][kNzMax];
 #pragma unroll
     for (int n = 0; n < NT; ++n)
@@ -466,28 +543,28 @@ __global__ void __launch_bounds__(128) k_cell_update(CellUpdateArgs a, int tr0) 
         const size_t f = (size_t)i + (size_t)(nx + 1) * j;
         const double kh = a.khtr_u ? __ldg(a.khtr_u + f) : a.khtr;
         const double coef = a.dt * kh * __ldg(a.dy_cu + f) * __ldg(a.idxCu + f);
-        face_accumulate<NT>(a, nt, tr0, a.u, f, ustride, col - 1, col, coef, false, dTr);
+        face_accumulate<NT>(a, nt, ti, pp, a.u, f, ustride, col - 1, col, coef, false, dTr);
     }
     // EAST u-face (face I+1): this cell is the LEFT column.
     if (I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e))) {
         const size_t f = (size_t)(i + 1) + (size_t)(nx + 1) * j;
         const double kh = a.khtr_u ? __ldg(a.khtr_u + f) : a.khtr;
         const double coef = a.dt * kh * __ldg(a.dy_cu + f) * __ldg(a.idxCu + f);
-        face_accumulate<NT>(a, nt, tr0, a.u, f, ustride, col, col + 1, coef, true, dTr);
+        face_accumulate<NT>(a, nt, ti, pp, a.u, f, ustride, col, col + 1, coef, true, dTr);
     }
     // SOUTH v-face (face J): this cell is the RIGHT (north) column.
     if (J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n))) {
         const size_t f = (size_t)i + (size_t)nx * j;
         const double kh = a.khtr_v ? __ldg(a.khtr_v + f) : a.khtr;
         const double coef = a.dt * kh * __ldg(a.dx_cv + f) * __ldg(a.idyCv + f);
-        face_accumulate<NT>(a, nt, tr0, a.v, f, vstride, col - nx, col, coef, false, dTr);
+        face_accumulate<NT>(a, nt, ti, pp, a.v, f, vstride, col - nx, col, coef, false, dTr);
     }
     // NORTH v-face (face J+1): this cell is the LEFT (south) column.
     if (J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))) {
         const size_t f = (size_t)i + (size_t)nx * (j + 1);
         const double kh = a.khtr_v ? __ldg(a.khtr_v + f) : a.khtr;
         const double coef = a.dt * kh * __ldg(a.dx_cv + f) * __ldg(a.idyCv + f);
-        face_accumulate<NT>(a, nt, tr0, a.v, f, vstride, col, col + nx, coef, true, dTr);
+        face_accumulate<NT>(a, nt, ti, pp, a.v, f, vstride, col, col + nx, coef, true, dTr);
     }
     const double iaij = 1.0 / __ldg(a.areaT + col);
 #pragma unroll

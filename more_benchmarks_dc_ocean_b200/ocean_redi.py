@@ -96,6 +96,7 @@ def lib() -> C.CDLL:
                                            vp, vp, C.POINTER(_BC), vp]
         L.redi_b200_get_coeffs.argtypes = [vp, C.POINTER(_Coeffs)]
         L.redi_b200_workspace_bytes.argtypes = [vp]
+        L.redi_b200_error_count.argtypes = [vp, C.c_int]
         L.redi_b200_workspace_bytes.restype = C.c_longlong
         L.redi_b200_last_error.restype = C.c_char_p
         L.redi_b200_version.restype = C.c_int
@@ -315,6 +316,10 @@ class OceanRedi:
         out["khtr_u"] = torch.as_tensor(_CudaArray(c.khtr_u, (ny, nx + 1), "<f8"), device="cuda")
         out["khtr_v"] = torch.as_tensor(_CudaArray(c.khtr_v, (ny + 1, nx), "<f8"), device="cuda")
         return out
+
+    def error_count(self, reset: bool = False) -> int:
+        """Out-of-order coefficient sublayers seen by Phase B (0 for sweep-produced coefficients)."""
+        return _check(lib().redi_b200_error_count(self._h, int(reset))) if self._h else 0
 
     def workspace_bytes(self) -> int:
         return int(lib().redi_b200_workspace_bytes(self._h)) if self._h else 0

@@ -52,6 +52,7 @@ def _run_gpu(p, nsteps, redi_lib, check_coeffs=True):
     torch.cuda.synchronize()
     coeffs = {k: v.cpu().numpy() for k, v in redi.coeffs().items()} if check_coeffs else None
     trs = [t.cpu().numpy() for t in dp.ms.tracers]
+    assert redi.error_count() == 0
     redi.destroy()
     return coeffs, trs
 
