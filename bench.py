@@ -49,8 +49,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Redi tracer-cell updates/s, HBM GB/s; mixed+batched vs FP64 plain, 1 B200"
 UNIT = "tracer-cell updates/s"
-KERNEL_NAMES = ["k_column_state", "k_neutral_sweep", "k_tracer_recon", "k_cell_update", "k_mixed_recon",
-                "k_mixed_cell_update", "k_mixed_sweep", "k_domain_persistent", "aux"]
+KERNEL_NAMES = ["k_column_state", "k_neutral_sweep", "k_tracer_recon", "k_cell_gather", "k_face_flux",
+                "k_mixed_recon", "k_mixed_flux", "k_mixed_sweep", "k_domain_persistent", "aux"]
+NKERN = len(KERNEL_NAMES)
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -102,12 +103,14 @@ def kernel_bytes(p, kid: int, precision: str = "fp64") -> float:
     face2d = 8 * (s["Fu"] + s["Fv"]) * 4 + 8 * s["ncol"]
     if kid == 0:   # column state: read h, T, S
         return 24.0 * s["Nt"]
-    if kid in (1, 6):  # neutral sweep: write the coefficients
+    if kid in (1, 7):  # neutral sweep: write the coefficients
         return float(bcoef)
-    if kid in (2, 4):  # tracer reconstruction: read h and every tracer
+    if kid in (2, 5):  # tracer reconstruction: read h and every tracer
         return 8.0 * s["Nt"] * (1 + s["ntr"])
-    if kid in (3, 5):  # cell update: read coefficients once, read+write every tracer
-        return float(bcoef + 16 * s["Nt"] * s["ntr"] + face2d)
+    if kid in (4, 6):  # face flux: read the coefficients once for every tracer
+        return float(bcoef + face2d)
+    if kid == 3:       # cell gather: read + write every tracer
+        return float(16 * s["Nt"] * s["ntr"] + 8 * s["ncol"])
     return 0.0
 
 
@@ -295,6 +298,16 @@ def run_b200(args, rank, world, local_rank):
         ex.setup_masks(dp, p.wet)
         ex.exchange()
     st = torch.cuda.current_stream()
+    tuning = None
+    if not args.no_tune:
+        from more_benchmarks_dc_ocean_b200 import autotune
+
+        tuning = autotune.tune(dp, redi, use_cache=False, stream=st)
+        if dist is not None:  # every rank uses rank 0's choice
+            t = torch.tensor(list(tuning["best"]), dtype=torch.int64, device=dev)
+            dist.broadcast(t, 0)
+            autotune.set_tuning(*[int(v) for v in t.tolist()])
+            tuning["best"] = tuple(int(v) for v in t.tolist())
     L = R.lib()
     L.redi_b200_launch_count.restype = C.c_ulonglong
     L.redi_b200_launch_count.argtypes = [C.c_int]
@@ -326,9 +339,9 @@ def run_b200(args, rank, world, local_rank):
     e1.record(st)
     torch.cuda.synchronize()
     n1 = L.redi_b200_launch_count(-1)
-    ktime = (C.c_double * 9)()
-    kcount = (C.c_ulonglong * 9)()
-    L.redi_b200_profile_end(ktime, kcount, 9)
+    ktime = (C.c_double * NKERN)()
+    kcount = (C.c_ulonglong * NKERN)()
+    L.redi_b200_profile_end(ktime, kcount, NKERN)
     barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / args.steps
@@ -337,8 +350,8 @@ def run_b200(args, rank, world, local_rank):
     upd_per_rank = p.ntr * p.nx_phys * p.ny_phys * p.nz
     value = upd_per_rank * world / (ms_all * 1e-3)
     kern = {KERNEL_NAMES[k]: {"ms_total": ktime[k], "launches": int(kcount[k]),
-                              "ms_per_launch": ktime[k] / kcount[k]} for k in range(9) if kcount[k]}
-    top = max((k for k in range(9) if kcount[k]), key=lambda k: ktime[k])
+                              "ms_per_launch": ktime[k] / kcount[k]} for k in range(NKERN) if kcount[k]}
+    top = max((k for k in range(NKERN) if kcount[k]), key=lambda k: ktime[k])
     peak, peak_kind = _peaks()
     bytes_launch = kernel_bytes(p, top, args.precision)
     t_launch = ktime[top] / kcount[top] * 1e-3
@@ -372,6 +385,8 @@ def run_b200(args, rank, world, local_rank):
             "e2e": e2e,
             "clocks": clk,
             "gpu_launches": int(n1 - n0),
+            "tuning": {"cell_update_tile": list(tuning["best"][:2]), "vertical_chunk": tuning["best"][2],
+                       "candidates_ms": tuning["ms"]} if tuning else None,
             "hbm_gbs_per_rank": bstep / (ms_all * 1e-3) / 1e9,
         }
         print(json.dumps(line), flush=True)
@@ -453,6 +468,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -157,14 +157,21 @@ REDI_B200_API const char* redi_b200_last_error(void);
 REDI_B200_API int redi_b200_version(void);
 
 /* Instrumentation (no counterpart in the reference). Kernel ids are
- * 0 column_state, 1 neutral_sweep, 2 tracer_recon, 3 cell_update,
- * 4 mixed_recon, 5 mixed_cell_update, 6 mixed_sweep, 7 domain_persistent,
- * 8 auxiliary; redi_b200_kernel_count() is their number.
+ * 0 column_state, 1 neutral_sweep, 2 tracer_recon, 3 cell_gather (the per-cell
+ * update), 4 face_flux, 5 mixed_recon, 6 mixed_flux, 7 mixed_sweep,
+ * 8 domain_persistent, 9 auxiliary; redi_b200_kernel_count() is their number.
  * redi_b200_launch_count(k) counts launches of kernel k since load (k < 0:
  * all). Between profile_begin and profile_end every launch is bracketed by a
  * CUDA event pair on its own stream; profile_end waits for them and returns,
  * per kernel id, the summed device time (ms) and the number of launches. */
 REDI_B200_API int redi_b200_kernel_count(void);
+
+/* Launch shape of the Phase-B cell update, process-wide (no counterpart in the
+ * reference): a bx x by tile of T-cell columns per block (bx*by a multiple of
+ * 32, at most 128) and the vertical chunk of layers processed per face pass
+ * (4, 8 or 16). Results do not depend on it; the autotuner picks it. */
+REDI_B200_API int redi_b200_set_tuning(int bx, int by, int chunk);
+REDI_B200_API int redi_b200_get_tuning(int* bx, int* by, int* chunk);
 REDI_B200_API unsigned long long redi_b200_launch_count(int kernel);
 REDI_B200_API int redi_b200_profile_begin(void);
 REDI_B200_API int redi_b200_profile_end(double* total_ms, unsigned long long* counts, int n);

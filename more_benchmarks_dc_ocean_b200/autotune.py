@@ -1,0 +1,125 @@
+"""Autotuner for the launch shape of the Phase-B cell update.
+
+The cell update is tiled as a bx x by block of T-cell columns and walks each
+column in vertical chunks of `chunk` layers (see csrc/redi_plain.cu). Results
+are identical for every choice; speed is not: the tile sets how many
+neighbouring columns and face rows a block shares through L1, the chunk sets
+the L2 working set between the W, E, S and N passes against the lane
+divergence at chunk edges. The tuner times every candidate on the live problem
+with the library's own CUDA-event launch timing and keeps the fastest,
+caching it per (GPU name, domain size class, nz, tracer count, precision) in a
+JSON file (``$REDI_B200_TUNING_CACHE`` or ``~/.cache/redi_b200/tuning.json``).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+from typing import Iterable, Optional, Sequence, Tuple
+
+TILES: Tuple[Tuple[int, int], ...] = ((32, 4), (64, 2), (128, 1), (32, 2), (32, 1))
+CHUNKS: Tuple[int, ...] = (4, 8, 16)
+K_CELL_UPDATE = 3
+
+
+def _cache_path() -> str:
+    return os.environ.get("REDI_B200_TUNING_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "redi_b200", "tuning.json"))
+
+
+def _bind(L):
+    L.redi_b200_set_tuning.argtypes = [C.c_int, C.c_int, C.c_int]
+    L.redi_b200_get_tuning.argtypes = [C.POINTER(C.c_int)] * 3
+    L.redi_b200_profile_end.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_ulonglong), C.c_int]
+    return L
+
+
+def get_tuning() -> Tuple[int, int, int]:
+    from . import ocean_redi as R
+
+    L = _bind(R.lib())
+    bx, by, ch = C.c_int(), C.c_int(), C.c_int()
+    R._check(L.redi_b200_get_tuning(C.byref(bx), C.byref(by), C.byref(ch)))
+    return bx.value, by.value, ch.value
+
+
+def set_tuning(bx: int, by: int, chunk: int) -> None:
+    from . import ocean_redi as R
+
+    R._check(_bind(R.lib()).redi_b200_set_tuning(int(bx), int(by), int(chunk)))
+
+
+def _key(dp, precision: int) -> str:
+    import torch
+
+    name = torch.cuda.get_device_name(dp.ms.h_layer.device)
+    cells = dp.grid.nx_total * dp.grid.ny_total
+    size_class = "large" if cells >= 1 << 20 else ("medium" if cells >= 1 << 16 else "small")
+    return f"{name}|{size_class}|nz{dp.ms.nz_ml}|ntr{len(dp.ms.tracers)}|p{precision}"
+
+
+def load_cached(dp, precision: int = 0) -> Optional[Tuple[int, int, int]]:
+    path = _cache_path()
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        v = d.get(_key(dp, precision))
+        return tuple(v) if v else None
+    except (OSError, ValueError):
+        return None
+
+
+def _store(dp, precision: int, best) -> None:
+    path = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        try:
+            with open(path) as f:
+                d = json.load(f)
+        except (OSError, ValueError):
+            d = {}
+        d[_key(dp, precision)] = list(best)
+        with open(path, "w") as f:
+            json.dump(d, f, indent=1)
+    except OSError:
+        pass
+
+
+def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, int, int]]] = None, reps: int = 2,
+         use_cache: bool = True, stream=None) -> dict:
+    """Time the cell update for every (bx, by, chunk) candidate and keep the fastest.
+
+    Runs redi_apply_flux on ``dp`` (its tracers are advanced in place). Returns
+    {"best": (bx, by, chunk), "ms": {candidate: ms per launch}, "cached": bool}.
+    """
+    import torch
+
+    from . import ocean_redi as R
+
+    prec = getattr(redi, "precision", 0)
+    if use_cache:
+        hit = load_cached(dp, prec)
+        if hit:
+            set_tuning(*hit)
+            return {"best": hit, "ms": {}, "cached": True}
+    L = _bind(R.lib())
+    cands = list(candidates) if candidates is not None else [(bx, by, c) for (bx, by) in TILES for c in CHUNKS]
+    R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, stream)
+    times = {}
+    for cand in cands:
+        set_tuning(*cand)
+        R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, stream)
+        torch.cuda.synchronize()
+        L.redi_b200_profile_begin()
+        for _ in range(reps):
+            R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, stream)
+        kt = (C.c_double * 16)()
+        kc = (C.c_ulonglong * 16)()
+        L.redi_b200_profile_end(kt, kc, 16)
+        kid = K_CELL_UPDATE
+        times[cand] = kt[kid] / max(1, kc[kid])
+    best = min(times, key=times.get)
+    set_tuning(*best)
+    _store(dp, prec, best)
+    return {"best": best, "ms": {f"{a}x{b}/ch{c}": round(v, 4) for (a, b, c), v in times.items()}, "cached": False}

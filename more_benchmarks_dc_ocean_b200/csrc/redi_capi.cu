@@ -132,27 +132,37 @@ struct PhaseBInputs {
 
 int run_plain_phase_b(const PhaseBInputs& in, int ntr, double* const* htr, Scratch& ws, cudaStream_t st) {
     const int group = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
-    cudaError_t e = ws.reserve(redi::plain_phase_b_scratch(in.nx, in.ny, in.nz, group));
+    const size_t recon = redi::plain_recon_bytes(in.nx, in.ny, in.nz, group);
+    const size_t flux = redi::plain_flux_bytes(in.nx, in.ny, in.nz, redi::kCellGroup);
+    cudaError_t e = ws.reserve(recon + flux);
     if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (phase B)");
     const size_t ncol = (size_t)in.nx * in.ny;
+    const size_t ns1 = (size_t)(2 * in.nz + 1);
+    double* Fu = reinterpret_cast<double*>(static_cast<char*>(ws.data()) + recon);
+    double* Fv = Fu + (size_t)redi::kCellGroup * ns1 * (size_t)(in.nx + 1) * in.ny;
     for (int t0 = 0; t0 < ntr; t0 += group) {
         const int nt = (ntr - t0) < group ? (ntr - t0) : group;
         redi::ReconArgs rc{};
         rc.nx = in.nx; rc.ny = in.ny; rc.nz = in.nz; rc.ntr = nt; rc.h = in.h;
         rc.ti = reinterpret_cast<double*>(ws.data());
         rc.ppm = reinterpret_cast<redi::PpmLayer*>(rc.ti + (size_t)nt * ncol * (in.nz + 1));
-        redi::CellUpdateArgs cu{};
-        cu.nx = in.nx; cu.ny = in.ny; cu.nz = in.nz; cu.ntr = nt;
-        cu.nghost = in.nghost; cu.nxp = in.nxp; cu.nyp = in.nyp;
-        cu.wall_w = in.walls[0]; cu.wall_e = in.walls[1]; cu.wall_s = in.walls[2]; cu.wall_n = in.walls[3];
-        cu.dt = in.dt; cu.khtr = in.khtr; cu.khtr_u = in.khtr_u; cu.khtr_v = in.khtr_v;
-        cu.dy_cu = in.dy_cu; cu.dx_cv = in.dx_cv; cu.idxCu = in.idxCu; cu.idyCv = in.idyCv; cu.areaT = in.areaT;
-        cu.u = in.u; cu.v = in.v; cu.ti = rc.ti; cu.ppm = rc.ppm; cu.err = ws.err();
+        redi::FaceFluxArgs ff{};
+        ff.nx = in.nx; ff.ny = in.ny; ff.nz = in.nz; ff.ntr = nt;
+        ff.nghost = in.nghost; ff.nxp = in.nxp; ff.nyp = in.nyp;
+        ff.wall_w = in.walls[0]; ff.wall_e = in.walls[1]; ff.wall_s = in.walls[2]; ff.wall_n = in.walls[3];
+        ff.dt = in.dt; ff.khtr = in.khtr; ff.khtr_u = in.khtr_u; ff.khtr_v = in.khtr_v;
+        ff.dy_cu = in.dy_cu; ff.dx_cv = in.dx_cv; ff.idxCu = in.idxCu; ff.idyCv = in.idyCv;
+        ff.u = in.u; ff.v = in.v; ff.ti = rc.ti; ff.ppm = rc.ppm; ff.Fu = Fu; ff.Fv = Fv;
+        redi::CellGatherArgs cg{};
+        cg.nx = in.nx; cg.ny = in.ny; cg.nz = in.nz; cg.ntr = nt;
+        cg.nghost = in.nghost; cg.nxp = in.nxp; cg.nyp = in.nyp;
+        cg.wall_w = in.walls[0]; cg.wall_e = in.walls[1]; cg.wall_s = in.walls[2]; cg.wall_n = in.walls[3];
+        cg.areaT = in.areaT; cg.u = in.u; cg.v = in.v; cg.Fu = Fu; cg.Fv = Fv; cg.err = ws.err();
         for (int n = 0; n < nt; ++n) {
             rc.htr[n] = htr[t0 + n];
-            cu.htr[n] = htr[t0 + n];
+            cg.htr[n] = htr[t0 + n];
         }
-        e = redi::launch_plain_phase_b(rc, cu, st);
+        e = redi::launch_plain_phase_b(rc, ff, cg, st);
         if (e != cudaSuccess) return cuda_fail(e, "phase B launch");
     }
     return REDI_B200_OK;
@@ -180,6 +190,10 @@ Profiler g_prof;
 }  // namespace
 
 namespace redi {
+static CellTuning g_cell_tuning{32, 4, 8};
+CellTuning cell_tuning() { return g_cell_tuning; }
+void set_cell_tuning(const CellTuning& t) { g_cell_tuning = t; }
+
 void launch_begin(int kid, cudaStream_t st) {
     std::lock_guard<std::mutex> lock(g_prof.mu);
     __atomic_add_fetch(&g_prof.launches[kid], 1ULL, __ATOMIC_RELAXED);
@@ -239,6 +253,22 @@ extern "C" {
 int redi_b200_version(void) { return 100; }
 
 int redi_b200_kernel_count(void) { return redi::K_NUM; }
+
+int redi_b200_set_tuning(int bx, int by, int chunk) {
+    if (bx < 1 || by < 1 || bx * by > 128 || (bx * by) % 32 != 0)
+        return fail(REDI_B200_E_ARG, "redi_b200_set_tuning: bx*by must be a multiple of 32 and at most 128");
+    if (chunk != 4 && chunk != 8 && chunk != 16)
+        return fail(REDI_B200_E_ARG, "redi_b200_set_tuning: chunk must be 4, 8 or 16");
+    redi::set_cell_tuning(redi::CellTuning{bx, by, chunk});
+    return REDI_B200_OK;
+}
+
+int redi_b200_get_tuning(int* bx, int* by, int* chunk) {
+    if (!bx || !by || !chunk) return fail(REDI_B200_E_ARG, "redi_b200_get_tuning: NULL argument");
+    const redi::CellTuning t = redi::cell_tuning();
+    *bx = t.bx; *by = t.by; *chunk = t.chunk;
+    return REDI_B200_OK;
+}
 
 unsigned long long redi_b200_launch_count(int kernel) {
     if (kernel < 0) {

@@ -55,7 +55,7 @@ struct ReconArgs {
     PpmLayer* ppm;   // [tracer][nz][column]
 };
 
-struct CellUpdateArgs {
+struct FaceFluxArgs {
     int nx, ny, nz, ntr;
     int nghost, nxp, nyp;
     int wall_w, wall_e, wall_s, wall_n;
@@ -67,12 +67,23 @@ struct CellUpdateArgs {
     const double* dx_cv;
     const double* idxCu;
     const double* idyCv;
-    const double* areaT;
     FaceIn u, v;
     const double* ti;       // [tracer][nz+1][column]
     const PpmLayer* ppm;    // [tracer][nz][column]
+    double* Fu;             // [group tracer][ns-1][(nx+1)*ny]
+    double* Fv;             // [group tracer][ns-1][nx*(ny+1)]
+};
+
+struct CellGatherArgs {
+    int nx, ny, nz, ntr;
+    int nghost, nxp, nyp;
+    int wall_w, wall_e, wall_s, wall_n;
+    const double* areaT;
+    FaceIn u, v;            // only KoL / KoR are read
+    const double* Fu;
+    const double* Fv;
     double* htr[kMaxTracers];
-    int* err;               // device error word (sublayers out of order), may be null
+    int* err;               // device error word (fluxes out of order), may be null
 };
 
 // Scratch bytes each phase needs for an (nx, ny, nz) domain with ntr tracers.
@@ -80,9 +91,13 @@ inline size_t plain_phase_a_scratch(int nx, int ny, int nz) {
     const size_t nifc = (size_t)nx * ny * (nz + 1);
     return nifc * sizeof(IfcState) + nifc * sizeof(double);
 }
-inline size_t plain_phase_b_scratch(int nx, int ny, int nz, int ntr) {
+inline size_t plain_recon_bytes(int nx, int ny, int nz, int ntr) {
     const size_t ncol = (size_t)nx * ny;
     return (size_t)ntr * ncol * ((nz + 1) * sizeof(double) + nz * sizeof(PpmLayer));
+}
+inline size_t plain_flux_bytes(int nx, int ny, int nz, int group) {
+    const size_t faces = (size_t)(nx + 1) * ny + (size_t)nx * (ny + 1);
+    return (size_t)group * (size_t)(2 * nz + 1) * faces * sizeof(double);
 }
 
 // Kernel identities for the launch counter and the optional event timing.
@@ -90,13 +105,14 @@ enum KernelId : int {
     K_COLUMN_STATE = 0,
     K_NEUTRAL_SWEEP = 1,
     K_TRACER_RECON = 2,
-    K_CELL_UPDATE = 3,
-    K_MIXED_RECON = 4,
-    K_MIXED_CELL_UPDATE = 5,
-    K_MIXED_SWEEP = 6,
-    K_DOMAIN_PERSISTENT = 7,
-    K_AUX = 8,
-    K_NUM = 9
+    K_CELL_UPDATE = 3,   // the per-cell gather
+    K_FACE_FLUX = 4,
+    K_MIXED_RECON = 5,
+    K_MIXED_FLUX = 6,
+    K_MIXED_SWEEP = 7,
+    K_DOMAIN_PERSISTENT = 8,
+    K_AUX = 9,
+    K_NUM = 10
 };
 
 // Launch bracketing: counts every kernel launch of the library and, while
@@ -105,7 +121,16 @@ enum KernelId : int {
 void launch_begin(int kid, cudaStream_t st);
 void launch_end(int kid, cudaStream_t st);
 
+// Launch shape of the FP64 cell update: a bx x by tile of columns per block
+// (bx * by <= 128) and the vertical chunk (layers per pass, 4, 8 or 16).
+struct CellTuning {
+    int bx, by, chunk;
+};
+CellTuning cell_tuning();
+void set_cell_tuning(const CellTuning& t);
+
 cudaError_t launch_plain_phase_a(const ColumnStateArgs& cs, const SweepArgs& sw, cudaStream_t st);
-cudaError_t launch_plain_phase_b(const ReconArgs& rc, const CellUpdateArgs& cu, cudaStream_t st);
+cudaError_t launch_plain_phase_b(const ReconArgs& rc, const FaceFluxArgs& ff, const CellGatherArgs& cg,
+                                 cudaStream_t st);
 
 }  // namespace redi

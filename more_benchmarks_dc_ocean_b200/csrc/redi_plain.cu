@@ -421,81 +421,112 @@ __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Phase B, step 2: per-cell flux divergence (redi_apply_flux_impl +
-// redi_face_flux + redi_sublayer_dT, ocean_redi.F90:893-925, 1037-1181).
+// Phase B, step 2: the along-neutral flux of every face, computed once
+// (redi_face_flux + redi_sublayer_dT, ocean_redi.F90:893-925, 1037-1092).
 //
-// One thread per T-cell column. The faces are visited in the reference order
-// W, E, S, N and, within a face, the sublayers ks = 1..ns-1 in order; all lanes
-// of a warp walk the same ks together, so the coefficient loads of a warp are
-// one contiguous row per array. Each contribution is added to the cell's dTr
-// entry for its native layer exactly as the reference adds it. The running
-// value of the current entry is held in a register while consecutive
-// sublayers hit the same layer (the cell-side Ko of a face is non-decreasing
-// in ks), and written back to the per-thread dTr array when the layer
-// changes: the same sequence of additions, with fewer local-memory accesses.
+// One thread per interior, non-wall face; all lanes of a warp walk the same
+// sublayer ks, so each coefficient load is one contiguous row. The flux
+// flx(ks) = dT * hEff * coef of every tracer is stored in F[tracer][ks][face];
+// sublayers with hEff == 0 store +0.0. The reference evaluates each interior
+// face twice (once from each adjacent cell, with identical operands and hence
+// identical bits); here it is evaluated once and read by both cells.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double interp(double P, double a, double b) { return (1.0 - P) * a + P * b; }
 
 template <int NT>
-__device__ __forceinline__ void face_accumulate(const CellUpdateArgs& a, int nt, const double* const (&ti)[NT],
-                                                const PpmLayer* const (&pp)[NT], const FaceIn& F, size_t fo,
-                                                size_t fstride, int colL, int colR, double coef, bool is_left,
-                                                double (&dTr)[NT][kNzMax]) {
-    const int nz = a.nz, ns = 2 * nz + 2;
-    const size_t ncol = (size_t)a.nx * a.ny;
-    const double* __restrict__ hEff = F.hEff + fo;
-    const double* __restrict__ PoL = F.PoL + fo;
-    const double* __restrict__ PoR = F.PoR + fo;
-    const int* __restrict__ KoL = F.KoL + fo;
-    const int* __restrict__ KoR = F.KoR + fo;
+__global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgs a, int tr0) {
+    const int dir = blockIdx.y;  // 0: u-faces, 1: v-faces
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    const size_t ncol = (size_t)nx * ny;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int colL, colR, fo;
+    size_t fstride;
+    if (dir == 0) {  // Fortran faces I = 2..nx, excluding walls
+        if (t >= (nx - 1) * ny) return;
+        const int j = t / (nx - 1), fi = 1 + t % (nx - 1);
+        const int I = fi + 1;
+        if ((a.wall_w && I == a.nghost + 1) || (a.wall_e && I == a.nghost + a.nxp + 1)) return;
+        colL = (fi - 1) + nx * j;
+        colR = fi + nx * j;
+        fo = fi + (nx + 1) * j;
+        fstride = (size_t)(nx + 1) * ny;
+    } else {  // Fortran faces J = 2..ny, excluding walls
+        if (t >= nx * (ny - 1)) return;
+        const int fj = 1 + t / nx, i = t % nx;
+        const int J = fj + 1;
+        if ((a.wall_s && J == a.nghost + 1) || (a.wall_n && J == a.nghost + a.nyp + 1)) return;
+        colL = i + nx * (fj - 1);
+        colR = i + nx * fj;
+        fo = i + nx * fj;
+        fstride = (size_t)nx * (ny + 1);
+    }
+    const FaceIn& c = dir == 0 ? a.u : a.v;
+    const double* __restrict__ hEff = c.hEff + fo;
+    const double* __restrict__ PoL = c.PoL + fo;
+    const double* __restrict__ PoR = c.PoR + fo;
+    const int* __restrict__ KoL = c.KoL + fo;
+    const int* __restrict__ KoR = c.KoR + fo;
+    const double* kh = dir == 0 ? a.khtr_u : a.khtr_v;
+    const double khv = kh ? __ldg(kh + fo) : a.khtr;
+    // ((dt*khtr)*dy)*idx, ocean_redi.F90:1156/1168
+    const double coef = a.dt * khv * __ldg((dir == 0 ? a.dy_cu : a.dx_cv) + fo) *
+                        __ldg((dir == 0 ? a.idxCu : a.idyCv) + fo);
+    const int nt = min(NT, a.ntr - tr0);
+    const double* tiL[NT];
+    const double* tiR[NT];
+    const PpmLayer* ppL[NT];
+    const PpmLayer* ppR[NT];
+    double* Fo[NT];
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        const int tr = tr0 + (n < nt ? n : 0);
+        tiL[n] = a.ti + (size_t)tr * ncol * (nz + 1) + colL;
+        tiR[n] = a.ti + (size_t)tr * ncol * (nz + 1) + colR;
+        ppL[n] = a.ppm + (size_t)tr * ncol * nz + colL;
+        ppR[n] = a.ppm + (size_t)tr * ncol * nz + colR;
+        Fo[n] = (dir == 0 ? a.Fu : a.Fv) + (size_t)(tr - tr0) * (size_t)(ns - 1) * fstride + fo;
+    }
 
     int cached = -1;  // surface whose tracer values are held in tl/tr
     int kl_t = 1, kr_t = 1;
     double pl_t = 0.0, pr_t = 0.0;
     double tl[NT], tr[NT];
-    int cur = -1;     // dTr entry held in acc
-    double acc[NT];
-
     for (int s = 0; s < ns - 1; ++s) {
-        const double he = __ldg(hEff + s * fstride);
-        if (he == 0.0) continue;
+        const size_t s0 = (size_t)s * fstride;
+        const double he = __ldg(hEff + s0);
+        if (he == 0.0) {
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+                if (n < nt) Fo[n][s0] = 0.0;
+            continue;
+        }
         if (cached != s) {
-            kl_t = min(max(__ldg(KoL + s * fstride), 1), nz);
-            kr_t = min(max(__ldg(KoR + s * fstride), 1), nz);
-            pl_t = __ldg(PoL + s * fstride);
-            pr_t = __ldg(PoR + s * fstride);
+            kl_t = min(max(__ldg(KoL + s0), 1), nz);
+            kr_t = min(max(__ldg(KoR + s0), 1), nz);
+            pl_t = __ldg(PoL + s0);
+            pr_t = __ldg(PoR + s0);
 #pragma unroll
             for (int n = 0; n < NT; ++n) {
-                tl[n] = interp(pl_t, __ldg(ti[n] + (size_t)(kl_t - 1) * ncol + colL), __ldg(ti[n] + (size_t)kl_t * ncol + colL));
-                tr[n] = interp(pr_t, __ldg(ti[n] + (size_t)(kr_t - 1) * ncol + colR), __ldg(ti[n] + (size_t)kr_t * ncol + colR));
+                tl[n] = interp(pl_t, __ldg(tiL[n] + (size_t)(kl_t - 1) * ncol), __ldg(tiL[n] + (size_t)kl_t * ncol));
+                tr[n] = interp(pr_t, __ldg(tiR[n] + (size_t)(kr_t - 1) * ncol), __ldg(tiR[n] + (size_t)kr_t * ncol));
             }
         }
-        const size_t s1 = (size_t)(s + 1) * fstride;
+        const size_t s1 = s0 + fstride;
         const int kl_b = min(max(__ldg(KoL + s1), 1), nz);
         const int kr_b = min(max(__ldg(KoR + s1), 1), nz);
         const double pl_b = __ldg(PoL + s1);
         const double pr_b = __ldg(PoR + s1);
         const double xRl = pl_b + (double)(kl_b - kl_t);
         const double xRr = pr_b + (double)(kr_b - kr_t);
-        const int knat = is_left ? nz - kl_t : nz - kr_t;
-        if (knat != cur) {
-#pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                if (cur >= 0) dTr[n][cur] = acc[n];
-                acc[n] = dTr[n][knat];
-            }
-            cur = knat;
-        }
 #pragma unroll
         for (int n = 0; n < NT; ++n) {
-            const double bl = interp(pl_b, __ldg(ti[n] + (size_t)(kl_b - 1) * ncol + colL), __ldg(ti[n] + (size_t)kl_b * ncol + colL));
-            const double br = interp(pr_b, __ldg(ti[n] + (size_t)(kr_b - 1) * ncol + colR), __ldg(ti[n] + (size_t)kr_b * ncol + colR));
+            const double bl = interp(pl_b, __ldg(tiL[n] + (size_t)(kl_b - 1) * ncol), __ldg(tiL[n] + (size_t)kl_b * ncol));
+            const double br = interp(pr_b, __ldg(tiR[n] + (size_t)(kr_b - 1) * ncol), __ldg(tiR[n] + (size_t)kr_b * ncol));
             if (n < nt) {
-                const double tlay = ppm_ave(pl_t, xRl, load_ppm(pp[n] + (size_t)(kl_t - 1) * ncol + colL));
-                const double trlay = ppm_ave(pr_t, xRr, load_ppm(pp[n] + (size_t)(kr_t - 1) * ncol + colR));
+                const double tlay = ppm_ave(pl_t, xRl, load_ppm(ppL[n] + (size_t)(kl_t - 1) * ncol));
+                const double trlay = ppm_ave(pr_t, xRr, load_ppm(ppR[n] + (size_t)(kr_t - 1) * ncol));
                 const double dT = guarded_dT(tr[n] - tl[n], br - bl, trlay - tlay);
-                const double flx = dT * he * coef;
-                acc[n] = is_left ? acc[n] + flx : acc[n] - flx;
+                Fo[n][s0] = dT * he * coef;
             }
             tl[n] = bl;
             tr[n] = br;
@@ -506,74 +537,127 @@ __device__ __forceinline__ void face_accumulate(const CellUpdateArgs& a, int nt,
         pl_t = pl_b;
         pr_t = pr_b;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Phase B, step 3: per-cell flux divergence (redi_apply_flux_impl,
+// ocean_redi.F90:1094-1181).
+//
+// One thread per T-cell column; a block is a BX x BY tile of columns. The
+// reference adds, for each native layer of a cell, the flux of the W face
+// (sublayers ks ascending, -flx into layer nz+1-KoR), then E (+flx at
+// nz+1-KoL), S (-flx at KoR) and N (+flx at KoL) to dTr(k) starting from
+// zero, then hTr(k) += dTr(k)*(1/areaT). Along one face the cell-side Ko is
+// non-decreasing in ks (the sweep's monotonic-position backstop,
+// ocean_redi.F90:385-388, 424-427), so one face's contributions to a block of
+// CH layers form a contiguous run of sublayers. The kernel walks the column in
+// chunks of CH layers and, per chunk, folds the W, E, S and N runs that land in
+// it, in that order: every layer receives exactly the reference's additions in
+// the reference's sequence (stored zero fluxes of skipped sublayers add +0.0,
+// which leaves any dTr value unchanged: dTr starts at +0.0 and an IEEE sum or
+// difference never turns it into -0.0). Consecutive additions to one layer run
+// in a register. A flux whose cell-side layer lies behind the chunk (not
+// possible for sweep-produced coefficients) is counted in the device error
+// word and skipped.
+// ---------------------------------------------------------------------------
+template <int NT, int CH>
+__device__ __forceinline__ void gather_run(const double* const (&F)[NT], const int* __restrict__ KoS, size_t stride,
+                                           bool left, int ns, int& ptr, int k0, int k1, double (&dTr)[NT][CH],
+                                           int& bad) {
+    int cur = -1;
+    double acc[NT];
+    int s = ptr;
+    for (; s < ns - 1; ++s) {
+        const size_t so = (size_t)s * stride;
+        const int k = __ldg(KoS + so);
+        if (k >= k1) break;
+        if (k < k0) {
+            ++bad;
+            continue;
+        }
+        const int slot = k - k0;
+        if (slot != cur) {
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                if (cur >= 0) dTr[n][cur] = acc[n];
+                acc[n] = dTr[n][slot];
+            }
+            cur = slot;
+        }
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            const double flx = __ldg(F[n] + so);
+            acc[n] = left ? acc[n] + flx : acc[n] - flx;
+        }
+    }
+    ptr = s;
     if (cur >= 0) {
 #pragma unroll
         for (int n = 0; n < NT; ++n) dTr[n][cur] = acc[n];
     }
 }
 
-template <int NT>
-__global__ void __launch_bounds__(128) k_cell_update(CellUpdateArgs a, int tr0) {
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int ncol = nx * ny;
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncol) return;
+template <int NT, int CH>
+__global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgs a, int tr0) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= nx || j >= ny) return;
+    const size_t ncol = (size_t)nx * ny;
+    const int col = i + nx * j;
     const int nt = min(NT, a.ntr - tr0);
-    const int i = col % nx, j = col / nx;
     const int I = i + 1, J = j + 1;  // Fortran indices
     const int wuf_w = a.nghost + 1, wuf_e = a.nghost + a.nxp + 1;
     const int wvf_s = a.nghost + 1, wvf_n = a.nghost + a.nyp + 1;
-
-    const double* ti[NT];
-    const PpmLayer* pp[NT];
-#pragma unroll
-    for (int n = 0; n < NT; ++n) {
-        const int tr = tr0 + (n < nt ? n : 0);
-        ti[n] = a.ti + (size_t)tr * ncol * (nz + 1);
-        pp[n] = a.ppm + (size_t)tr * ncol * nz;
-    }
-    double dTr[NT][kNzMax];
-#pragma unroll
-    for (int n = 0; n < NT; ++n)
-        for (int k = 0; k < nz; ++k) dTr[n][k] = 0.0;
-
     const size_t ustride = (size_t)(nx + 1) * ny, vstride = (size_t)nx * (ny + 1);
-    // WEST u-face (face I): this cell is the RIGHT column.
-    if (I >= 2 && !((a.wall_w && I == wuf_w) || (a.wall_e && I == wuf_e))) {
-        const size_t f = (size_t)i + (size_t)(nx + 1) * j;
-        const double kh = a.khtr_u ? __ldg(a.khtr_u + f) : a.khtr;
-        const double coef = a.dt * kh * __ldg(a.dy_cu + f) * __ldg(a.idxCu + f);
-        face_accumulate<NT>(a, nt, ti, pp, a.u, f, ustride, col - 1, col, coef, false, dTr);
-    }
-    // EAST u-face (face I+1): this cell is the LEFT column.
-    if (I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e))) {
-        const size_t f = (size_t)(i + 1) + (size_t)(nx + 1) * j;
-        const double kh = a.khtr_u ? __ldg(a.khtr_u + f) : a.khtr;
-        const double coef = a.dt * kh * __ldg(a.dy_cu + f) * __ldg(a.idxCu + f);
-        face_accumulate<NT>(a, nt, ti, pp, a.u, f, ustride, col, col + 1, coef, true, dTr);
-    }
-    // SOUTH v-face (face J): this cell is the RIGHT (north) column.
-    if (J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n))) {
-        const size_t f = (size_t)i + (size_t)nx * j;
-        const double kh = a.khtr_v ? __ldg(a.khtr_v + f) : a.khtr;
-        const double coef = a.dt * kh * __ldg(a.dx_cv + f) * __ldg(a.idyCv + f);
-        face_accumulate<NT>(a, nt, ti, pp, a.v, f, vstride, col - nx, col, coef, false, dTr);
-    }
-    // NORTH v-face (face J+1): this cell is the LEFT (south) column.
-    if (J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))) {
-        const size_t f = (size_t)i + (size_t)nx * (j + 1);
-        const double kh = a.khtr_v ? __ldg(a.khtr_v + f) : a.khtr;
-        const double coef = a.dt * kh * __ldg(a.dx_cv + f) * __ldg(a.idyCv + f);
-        face_accumulate<NT>(a, nt, ti, pp, a.v, f, vstride, col, col + nx, coef, true, dTr);
-    }
+    // Faces in the reference order: W (u-face I, this cell RIGHT), E (u-face
+    // I+1, LEFT), S (v-face J, RIGHT), N (v-face J+1, LEFT).
+    const bool on[4] = {I >= 2 && !((a.wall_w && I == wuf_w) || (a.wall_e && I == wuf_e)),
+                        I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e)),
+                        J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n)),
+                        J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))};
+    const int fo[4] = {i + (nx + 1) * j, i + 1 + (nx + 1) * j, i + nx * j, i + nx * (j + 1)};
     const double iaij = 1.0 / __ldg(a.areaT + col);
+    int ptr[4] = {0, 0, 0, 0};
+    int bad = 0;
+    double dTr[NT][CH];
+    for (int k0 = 1; k0 <= nz; k0 += CH) {
+        const int k1 = min(k0 + CH, nz + 1);
 #pragma unroll
-    for (int n = 0; n < NT; ++n) {
-        if (n < nt) {
+        for (int n = 0; n < NT; ++n)
+#pragma unroll
+            for (int c = 0; c < CH; ++c) dTr[n][c] = 0.0;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            if (!on[f]) continue;
+            const bool u = f < 2, left = (f & 1) != 0;
+            const size_t stride = u ? ustride : vstride;
+            const double* F[NT];
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+                F[n] = (u ? a.Fu : a.Fv) + (size_t)(n < nt ? n : 0) * (size_t)(ns - 1) * stride + fo[f];
+            const FaceIn& c = u ? a.u : a.v;
+            gather_run<NT, CH>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1, dTr, bad);
+        }
+        // Layers k0..k1-1 are complete: hTr(knat) += dTr(knat) * (1/areaT), knat = nz + 1 - k.
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            if (n >= nt) break;
             double* __restrict__ out = a.htr[tr0 + n] + col;
-            for (int k = 0; k < nz; ++k) out[(size_t)k * ncol] = out[(size_t)k * ncol] + dTr[n][k] * iaij;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const int k = k0 + c;
+                if (k < k1) {
+                    const size_t o = (size_t)(nz - k) * ncol;
+                    out[o] = out[o] + dTr[n][c] * iaij;
+                }
+            }
         }
     }
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+        if (on[f] && ptr[f] < ns - 1) ++bad;  // fluxes whose cell-side layer is beyond nz
+    if (bad && a.err) atomicAdd(a.err, bad);
 }
 
 }  // namespace plain
@@ -596,7 +680,8 @@ cudaError_t launch_plain_phase_a(const ColumnStateArgs& cs, const SweepArgs& sw,
     return cudaGetLastError();
 }
 
-cudaError_t launch_plain_phase_b(const ReconArgs& rc, const CellUpdateArgs& cu, cudaStream_t st) {
+cudaError_t launch_plain_phase_b(const ReconArgs& rc, const FaceFluxArgs& ff, const CellGatherArgs& cg,
+                                 cudaStream_t st) {
     const int ncol = rc.nx * rc.ny;
     // Reconstruct in groups of two tracers (register window of 2 scalars).
     {
@@ -606,10 +691,22 @@ cudaError_t launch_plain_phase_b(const ReconArgs& rc, const CellUpdateArgs& cu, 
         plain::k_tracer_recon<2><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc);
         launch_end(K_TRACER_RECON, st);
     }
-    // Update in groups of up to kCellGroup tracers.
-    for (int tr0 = 0; tr0 < cu.ntr; tr0 += kCellGroup) {
+    const CellTuning tune = cell_tuning();
+    const dim3 block(tune.bx, tune.by);
+    const dim3 cgrid((cg.nx + tune.bx - 1) / tune.bx, (cg.ny + tune.by - 1) / tune.by);
+    const int nface = max((ff.nx - 1) * ff.ny, ff.nx * (ff.ny - 1));
+    for (int tr0 = 0; tr0 < ff.ntr; tr0 += kCellGroup) {
+        if (nface > 0) {
+            launch_begin(K_FACE_FLUX, st);
+            plain::k_face_flux<kCellGroup><<<dim3((nface + 127) / 128, 2), 128, 0, st>>>(ff, tr0);
+            launch_end(K_FACE_FLUX, st);
+        }
         launch_begin(K_CELL_UPDATE, st);
-        plain::k_cell_update<kCellGroup><<<(ncol + 127) / 128, 128, 0, st>>>(cu, tr0);
+        switch (tune.chunk) {
+            case 4: plain::k_cell_gather<kCellGroup, 4><<<cgrid, block, 0, st>>>(cg, tr0); break;
+            case 16: plain::k_cell_gather<kCellGroup, 16><<<cgrid, block, 0, st>>>(cg, tr0); break;
+            default: plain::k_cell_gather<kCellGroup, 8><<<cgrid, block, 0, st>>>(cg, tr0); break;
+        }
         launch_end(K_CELL_UPDATE, st);
     }
     return cudaGetLastError();

@@ -201,3 +201,36 @@ def test_invalid_arguments_raise(redi_lib):
     redi.destroy()
     with pytest.raises(R.RediError):
         R.OceanRedi().init(dp.grid, 4096)
+
+
+@pytest.mark.parametrize("tile,chunk", [((32, 4), 4), ((64, 2), 8), ((128, 1), 16), ((32, 1), 8)])
+def test_cell_update_launch_shapes_are_bit_identical(redi_lib, oracle_lib, tile, chunk):
+    """Every tile shape and vertical chunk of the cell update gives the reference's result."""
+    from more_benchmarks_dc_ocean_b200 import autotune
+
+    saved = autotune.get_tuning()
+    try:
+        autotune.set_tuning(tile[0], tile[1], chunk)
+        _compare(inputs.make_problem(37, 29, 23, n_passive=1, seed=31), 2, redi_lib)
+    finally:
+        autotune.set_tuning(*saved)
+
+
+def test_autotuner_picks_a_candidate(redi_lib, tmp_path, monkeypatch):
+    from more_benchmarks_dc_ocean_b200 import autotune
+
+    monkeypatch.setenv("REDI_B200_TUNING_CACHE", str(tmp_path / "t.json"))
+    saved = autotune.get_tuning()
+    try:
+        p = inputs.make_problem(40, 30, 12, seed=4)
+        R = redi_lib
+        dp = R.to_device(p)
+        redi = R.make_redi(dp)
+        res = autotune.tune(dp, redi, candidates=[(32, 4, 8), (64, 2, 4)], reps=1)
+        assert res["best"] in [(32, 4, 8), (64, 2, 4)] and not res["cached"]
+        assert autotune.get_tuning() == res["best"]
+        again = autotune.tune(dp, redi, candidates=[(32, 4, 8), (64, 2, 4)], reps=1)
+        assert again["cached"] and again["best"] == res["best"]
+        redi.destroy()
+    finally:
+        autotune.set_tuning(*saved)
