@@ -51,6 +51,15 @@ cudaError_t fill_int(int* p, size_t n, int v, cudaStream_t st) {
     k_fill_int<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, v);
     return cudaGetLastError();
 }
+__global__ void k_fill_short(int16_t* p, size_t n, int16_t v) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t < n) p[t] = v;
+}
+cudaError_t fill_short(int16_t* p, size_t n, int16_t v, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_fill_short<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, v);
+    return cudaGetLastError();
+}
 
 // Grow-only device scratch. The first 256 bytes hold the device error word
 // (count of out-of-order coefficient sublayers seen by the cell update); phase
@@ -101,11 +110,12 @@ bool dims_ok(int nx, int ny, int nz, std::string& why) {
     return true;
 }
 
-// Phase A on FP64 slots with caller-provided or handle-owned arrays.
-int run_plain_phase_a(int nx, int ny, int nz, const redi::EosLin& eos, const double* h, const double* th,
-                      const double* sh, const double* wet_u, const double* wet_v, const redi::FaceOut& u,
-                      const redi::FaceOut& v, Scratch& ws, cudaStream_t st) {
-    cudaError_t e = ws.reserve(redi::plain_phase_a_scratch(nx, ny, nz));
+// Phase A into caller-provided or handle-owned coefficient slots.
+template <class P>
+int run_phase_a(int nx, int ny, int nz, const redi::EosLin& eos, const double* h, const double* th,
+                const double* sh, const double* wet_u, const double* wet_v, const redi::FaceOutT<P>& u,
+                const redi::FaceOutT<P>& v, Scratch& ws, cudaStream_t st) {
+    cudaError_t e = ws.reserve(redi::phase_a_scratch(nx, ny, nz));
     if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (phase A)");
     const size_t nifc = (size_t)nx * ny * (nz + 1);
     redi::ColumnStateArgs cs{};
@@ -113,47 +123,51 @@ int run_plain_phase_a(int nx, int ny, int nz, const redi::EosLin& eos, const dou
     cs.h = h; cs.th = th; cs.sh = sh;
     cs.ifc = reinterpret_cast<redi::IfcState*>(ws.data());
     cs.pint = reinterpret_cast<double*>(cs.ifc + nifc);
-    redi::SweepArgs sw{};
+    redi::SweepArgsT<P> sw{};
     sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos.rho0;
     sw.wet_u = wet_u; sw.wet_v = wet_v; sw.ifc = cs.ifc; sw.pint = cs.pint;
     sw.u = u; sw.v = v;
-    e = redi::launch_plain_phase_a(cs, sw, st);
+    e = redi::launch_column_state(cs, st);
+    if (e == cudaSuccess) e = redi::launch_sweep<P>(sw, st);
     if (e != cudaSuccess) return cuda_fail(e, "phase A launch");
     return REDI_B200_OK;
 }
 
+template <class P>
 struct PhaseBInputs {
     int nx, ny, nz, nghost, nxp, nyp;
     int walls[4];
     double dt, khtr;
     const double *khtr_u, *khtr_v, *dy_cu, *dx_cv, *idxCu, *idyCv, *areaT, *h;
-    redi::FaceIn u, v;
+    redi::FaceInT<P> u, v;
 };
 
-int run_plain_phase_b(const PhaseBInputs& in, int ntr, double* const* htr, Scratch& ws, cudaStream_t st) {
-    const int group = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
-    const size_t recon = redi::plain_recon_bytes(in.nx, in.ny, in.nz, group);
-    const size_t flux = redi::plain_flux_bytes(in.nx, in.ny, in.nz, redi::kCellGroup);
+template <class P>
+int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch& ws, cudaStream_t st) {
+    const int batch = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
+    const size_t recon = redi::recon_bytes<P>(in.nx, in.ny, in.nz, batch);
+    const size_t flux = redi::flux_bytes<P>(in.nx, in.ny, in.nz, redi::tracer_group(batch));
     cudaError_t e = ws.reserve(recon + flux);
     if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (phase B)");
     const size_t ncol = (size_t)in.nx * in.ny;
     const size_t ns1 = (size_t)(2 * in.nz + 1);
-    double* Fu = reinterpret_cast<double*>(static_cast<char*>(ws.data()) + recon);
-    double* Fv = Fu + (size_t)redi::kCellGroup * ns1 * (size_t)(in.nx + 1) * in.ny;
-    for (int t0 = 0; t0 < ntr; t0 += group) {
-        const int nt = (ntr - t0) < group ? (ntr - t0) : group;
-        redi::ReconArgs rc{};
+    using Flux = typename P::Flux;
+    Flux* Fu = reinterpret_cast<Flux*>(static_cast<char*>(ws.data()) + recon);
+    Flux* Fv = Fu + (size_t)redi::tracer_group(batch) * ns1 * (size_t)(in.nx + 1) * in.ny;
+    for (int t0 = 0; t0 < ntr; t0 += batch) {
+        const int nt = (ntr - t0) < batch ? (ntr - t0) : batch;
+        redi::ReconArgsT<P> rc{};
         rc.nx = in.nx; rc.ny = in.ny; rc.nz = in.nz; rc.ntr = nt; rc.h = in.h;
         rc.ti = reinterpret_cast<double*>(ws.data());
-        rc.ppm = reinterpret_cast<redi::PpmLayer*>(rc.ti + (size_t)nt * ncol * (in.nz + 1));
-        redi::FaceFluxArgs ff{};
+        rc.ppm = reinterpret_cast<typename P::Ppm*>(rc.ti + (size_t)nt * ncol * (in.nz + 1));
+        redi::FaceFluxArgsT<P> ff{};
         ff.nx = in.nx; ff.ny = in.ny; ff.nz = in.nz; ff.ntr = nt;
         ff.nghost = in.nghost; ff.nxp = in.nxp; ff.nyp = in.nyp;
         ff.wall_w = in.walls[0]; ff.wall_e = in.walls[1]; ff.wall_s = in.walls[2]; ff.wall_n = in.walls[3];
         ff.dt = in.dt; ff.khtr = in.khtr; ff.khtr_u = in.khtr_u; ff.khtr_v = in.khtr_v;
         ff.dy_cu = in.dy_cu; ff.dx_cv = in.dx_cv; ff.idxCu = in.idxCu; ff.idyCv = in.idyCv;
         ff.u = in.u; ff.v = in.v; ff.ti = rc.ti; ff.ppm = rc.ppm; ff.Fu = Fu; ff.Fv = Fv;
-        redi::CellGatherArgs cg{};
+        redi::CellGatherArgsT<P> cg{};
         cg.nx = in.nx; cg.ny = in.ny; cg.nz = in.nz; cg.ntr = nt;
         cg.nghost = in.nghost; cg.nxp = in.nxp; cg.nyp = in.nyp;
         cg.wall_w = in.walls[0]; cg.wall_e = in.walls[1]; cg.wall_s = in.walls[2]; cg.wall_n = in.walls[3];
@@ -162,7 +176,7 @@ int run_plain_phase_b(const PhaseBInputs& in, int ntr, double* const* htr, Scrat
             rc.htr[n] = htr[t0 + n];
             cg.htr[n] = htr[t0 + n];
         }
-        e = redi::launch_plain_phase_b(rc, ff, cg, st);
+        e = redi::launch_phase_b<P>(rc, ff, cg, st);
         if (e != cudaSuccess) return cuda_fail(e, "phase B launch");
     }
     return REDI_B200_OK;
@@ -227,12 +241,32 @@ struct redi_b200 {
     int nx_total = 0, ny_total = 0, nz_ml = 0, nsurf = 0;
     int precision = REDI_B200_FP64;
     int device = -1;
-    // FP64 coefficient slots (ocean_redi.F90:105-116).
-    double *uPoL = nullptr, *uPoR = nullptr, *uhEff = nullptr;
-    int *uKoL = nullptr, *uKoR = nullptr;
-    double *vPoL = nullptr, *vPoR = nullptr, *vhEff = nullptr;
-    int *vKoL = nullptr, *vKoR = nullptr;
+    // Coefficient slots (ocean_redi.F90:105-116): Po f64, Ko i32 (FP64) or
+    // i16 (MIXED), hEff f64 (FP64) or f32 (MIXED).
+    double *uPoL = nullptr, *uPoR = nullptr, *vPoL = nullptr, *vPoR = nullptr;
+    void *uKoL = nullptr, *uKoR = nullptr, *vKoL = nullptr, *vKoR = nullptr;
+    void *uhEff = nullptr, *vhEff = nullptr;
     double *khtr_u = nullptr, *khtr_v = nullptr;
+    template <class P>
+    redi::FaceOutT<P> out_u() {
+        return {uPoL, uPoR, static_cast<typename P::Ko*>(uKoL), static_cast<typename P::Ko*>(uKoR),
+                static_cast<typename P::He*>(uhEff)};
+    }
+    template <class P>
+    redi::FaceOutT<P> out_v() {
+        return {vPoL, vPoR, static_cast<typename P::Ko*>(vKoL), static_cast<typename P::Ko*>(vKoR),
+                static_cast<typename P::He*>(vhEff)};
+    }
+    template <class P>
+    redi::FaceInT<P> in_u() {
+        auto o = out_u<P>();
+        return {o.PoL, o.PoR, o.KoL, o.KoR, o.hEff};
+    }
+    template <class P>
+    redi::FaceInT<P> in_v() {
+        auto o = out_v<P>();
+        return {o.PoL, o.PoR, o.KoL, o.KoR, o.hEff};
+    }
     Scratch ws;
     std::vector<void*> allocations;
 
@@ -321,8 +355,6 @@ int redi_b200_init(const redi_b200_grid* grid, int nz_ml, int precision, redi_b2
     if (!dims_ok(grid->nx_total, grid->ny_total, nz, why)) {
         return fail(nz > redi::kNzMax ? REDI_B200_E_UNSUPPORTED : REDI_B200_E_ARG, "redi_b200_init: " + why);
     }
-    if (precision == REDI_B200_MIXED)
-        return fail(REDI_B200_E_UNSUPPORTED, "redi_b200_init: the mixed-precision form is not built in this library");
     redi_b200* s = new (std::nothrow) redi_b200();
     if (!s) return fail(REDI_B200_E_NOMEM, "redi_b200_init: host allocation failed");
     cudaGetDevice(&s->device);
@@ -331,10 +363,11 @@ int redi_b200_init(const redi_b200_grid* grid, int nz_ml, int precision, redi_b2
     const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
     cudaError_t e = cudaSuccess;
     auto A = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = s->alloc(p, bytes); };
-    A((void**)&s->uPoL, nu * ns * 8); A((void**)&s->uPoR, nu * ns * 8); A((void**)&s->uhEff, nu * (ns - 1) * 8);
-    A((void**)&s->uKoL, nu * ns * 4); A((void**)&s->uKoR, nu * ns * 4);
-    A((void**)&s->vPoL, nv * ns * 8); A((void**)&s->vPoR, nv * ns * 8); A((void**)&s->vhEff, nv * (ns - 1) * 8);
-    A((void**)&s->vKoL, nv * ns * 4); A((void**)&s->vKoR, nv * ns * 4);
+    const size_t kb = precision == REDI_B200_FP64 ? 4 : 2, hb = precision == REDI_B200_FP64 ? 8 : 4;
+    A((void**)&s->uPoL, nu * ns * 8); A((void**)&s->uPoR, nu * ns * 8); A(&s->uhEff, nu * (ns - 1) * hb);
+    A(&s->uKoL, nu * ns * kb); A(&s->uKoR, nu * ns * kb);
+    A((void**)&s->vPoL, nv * ns * 8); A((void**)&s->vPoR, nv * ns * 8); A(&s->vhEff, nv * (ns - 1) * hb);
+    A(&s->vKoL, nv * ns * kb); A(&s->vKoR, nv * ns * kb);
     A((void**)&s->khtr_u, nu * 8); A((void**)&s->khtr_v, nv * 8);
     if (e != cudaSuccess) {
         s->free_all();
@@ -344,11 +377,16 @@ int redi_b200_init(const redi_b200_grid* grid, int nz_ml, int precision, redi_b2
     // ocean_redi.F90:493-505: Po = 0, Ko = 1, hEff = 0, khtr_* = 0.
     cudaStream_t st = 0;
     cudaMemsetAsync(s->uPoL, 0, nu * ns * 8, st); cudaMemsetAsync(s->uPoR, 0, nu * ns * 8, st);
-    cudaMemsetAsync(s->uhEff, 0, nu * (ns - 1) * 8, st);
+    cudaMemsetAsync(s->uhEff, 0, nu * (ns - 1) * hb, st);
     cudaMemsetAsync(s->vPoL, 0, nv * ns * 8, st); cudaMemsetAsync(s->vPoR, 0, nv * ns * 8, st);
-    cudaMemsetAsync(s->vhEff, 0, nv * (ns - 1) * 8, st);
-    fill_int(s->uKoL, nu * ns, 1, st); fill_int(s->uKoR, nu * ns, 1, st);
-    fill_int(s->vKoL, nv * ns, 1, st); fill_int(s->vKoR, nv * ns, 1, st);
+    cudaMemsetAsync(s->vhEff, 0, nv * (ns - 1) * hb, st);
+    if (precision == REDI_B200_FP64) {
+        fill_int((int*)s->uKoL, nu * ns, 1, st); fill_int((int*)s->uKoR, nu * ns, 1, st);
+        fill_int((int*)s->vKoL, nv * ns, 1, st); fill_int((int*)s->vKoR, nv * ns, 1, st);
+    } else {
+        fill_short((int16_t*)s->uKoL, nu * ns, 1, st); fill_short((int16_t*)s->uKoR, nu * ns, 1, st);
+        fill_short((int16_t*)s->vKoL, nv * ns, 1, st); fill_short((int16_t*)s->vKoR, nv * ns, 1, st);
+    }
     cudaMemsetAsync(s->khtr_u, 0, nu * 8, st);
     cudaMemsetAsync(s->khtr_v, 0, nv * 8, st);
     cudaError_t e2 = cudaStreamSynchronize(st);
@@ -389,8 +427,10 @@ int redi_b200_get_coeffs(const redi_b200* s, redi_b200_coeffs* out) {
     if (!s || !out) return fail(REDI_B200_E_ARG, "redi_b200_get_coeffs: NULL argument");
     if (s->precision != REDI_B200_FP64)
         return fail(REDI_B200_E_STATE, "redi_b200_get_coeffs: mixed-precision handles keep packed coefficients");
-    out->uPoL = s->uPoL; out->uPoR = s->uPoR; out->uhEff = s->uhEff; out->uKoL = s->uKoL; out->uKoR = s->uKoR;
-    out->vPoL = s->vPoL; out->vPoR = s->vPoR; out->vhEff = s->vhEff; out->vKoL = s->vKoL; out->vKoR = s->vKoR;
+    out->uPoL = s->uPoL; out->uPoR = s->uPoR; out->uhEff = (double*)s->uhEff;
+    out->uKoL = (int*)s->uKoL; out->uKoR = (int*)s->uKoR;
+    out->vPoL = s->vPoL; out->vPoR = s->vPoR; out->vhEff = (double*)s->vhEff;
+    out->vKoL = (int*)s->vKoL; out->vKoR = (int*)s->vKoR;
     out->khtr_u = s->khtr_u; out->khtr_v = s->khtr_v; out->nsurf = s->nsurf;
     return REDI_B200_OK;
 }
@@ -430,9 +470,11 @@ int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* m
         return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: misaligned device array");
     redi::EosLin e{eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    redi::FaceOut u{s->uPoL, s->uPoR, s->uKoL, s->uKoR, s->uhEff};
-    redi::FaceOut v{s->vPoL, s->vPoR, s->vKoL, s->vKoR, s->vhEff};
-    return run_plain_phase_a(nx, ny, nz, e, ms->h_layer, th, sh, metrics->wet_u, metrics->wet_v, u, v, s->ws, st);
+    if (s->precision == REDI_B200_MIXED)
+        return run_phase_a<redi::MixedPrec>(nx, ny, nz, e, ms->h_layer, th, sh, metrics->wet_u, metrics->wet_v,
+                                            s->out_u<redi::MixedPrec>(), s->out_v<redi::MixedPrec>(), s->ws, st);
+    return run_phase_a<redi::PlainPrec>(nx, ny, nz, e, ms->h_layer, th, sh, metrics->wet_u, metrics->wet_v,
+                                        s->out_u<redi::PlainPrec>(), s->out_v<redi::PlainPrec>(), s->ws, st);
 }
 
 int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* metrics, redi_b200* s,
@@ -476,15 +518,25 @@ int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* me
         if (e == cudaSuccess) e = fill(s->khtr_v, nv, s->khtr, st);
     }
     if (e != cudaSuccess) return cuda_fail(e, "redi_b200_apply_flux: khtr resolve");
-    PhaseBInputs in{};
-    in.nx = nx; in.ny = ny; in.nz = nz; in.nghost = grid->nghost; in.nxp = grid->nx_phys; in.nyp = grid->ny_phys;
-    for (int w = 0; w < 4; ++w) in.walls[w] = walls[w];
-    in.dt = dt; in.khtr = s->khtr; in.khtr_u = s->khtr_u; in.khtr_v = s->khtr_v;
-    in.dy_cu = metrics->dy_cu; in.dx_cv = metrics->dx_cv; in.idxCu = metrics->idxCu; in.idyCv = metrics->idyCv;
-    in.areaT = metrics->areaT; in.h = ms->h_layer;
-    in.u = redi::FaceIn{s->uPoL, s->uPoR, s->uKoL, s->uKoR, s->uhEff};
-    in.v = redi::FaceIn{s->vPoL, s->vPoR, s->vKoL, s->vKoR, s->vhEff};
-    return run_plain_phase_b(in, ms->ntracers, ms->hTr, s->ws, st);
+    auto fill_in = [&](auto& in) {
+        in.nx = nx; in.ny = ny; in.nz = nz; in.nghost = grid->nghost; in.nxp = grid->nx_phys; in.nyp = grid->ny_phys;
+        for (int w = 0; w < 4; ++w) in.walls[w] = walls[w];
+        in.dt = dt; in.khtr = s->khtr; in.khtr_u = s->khtr_u; in.khtr_v = s->khtr_v;
+        in.dy_cu = metrics->dy_cu; in.dx_cv = metrics->dx_cv; in.idxCu = metrics->idxCu; in.idyCv = metrics->idyCv;
+        in.areaT = metrics->areaT; in.h = ms->h_layer;
+    };
+    if (s->precision == REDI_B200_MIXED) {
+        PhaseBInputs<redi::MixedPrec> in{};
+        fill_in(in);
+        in.u = s->in_u<redi::MixedPrec>();
+        in.v = s->in_v<redi::MixedPrec>();
+        return run_phase_b<redi::MixedPrec>(in, ms->ntracers, ms->hTr, s->ws, st);
+    }
+    PhaseBInputs<redi::PlainPrec> in{};
+    fill_in(in);
+    in.u = s->in_u<redi::PlainPrec>();
+    in.v = s->in_v<redi::PlainPrec>();
+    return run_phase_b<redi::PlainPrec>(in, ms->ntracers, ms->hTr, s->ws, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -528,12 +580,12 @@ static void compat_launch(const char* name, const int* nx_, const int* ny_, cons
     cudaStream_t st = 0;  // the reference launches on the legacy default stream
     redi::EosLin e{*rho0_, *T_ref_, *S_ref_, *alpha_T_, *beta_S_};
     redi::FaceOut u{uPoL, uPoR, uKoL, uKoR, uhEff}, v{vPoL, vPoR, vKoL, vKoR, vhEff};
-    int rc = run_plain_phase_a(nx, ny, nz, e, h_layer, t_htr, s_htr, wet_u, wet_v, u, v, ws, st);
+    int rc = run_phase_a<redi::PlainPrec>(nx, ny, nz, e, h_layer, t_htr, s_htr, wet_u, wet_v, u, v, ws, st);
     if (rc < 0) { report(rc, g_last_error); return; }
     const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
     cudaMemcpyAsync(khtr_u, khtr_u_ext, nu * 8, cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(khtr_v, khtr_v_ext, nv * 8, cudaMemcpyDeviceToDevice, st);
-    PhaseBInputs in{};
+    PhaseBInputs<redi::PlainPrec> in{};
     in.nx = nx; in.ny = ny; in.nz = nz; in.nghost = *nghost_; in.nxp = *nxp_; in.nyp = *nyp_;
     in.walls[0] = *ww_; in.walls[1] = *we_; in.walls[2] = *wsz_; in.walls[3] = *wn_;
     in.dt = *dt_; in.khtr = 0.0; in.khtr_u = khtr_u; in.khtr_v = khtr_v;
@@ -541,7 +593,7 @@ static void compat_launch(const char* name, const int* nx_, const int* ny_, cons
     in.u = redi::FaceIn{uPoL, uPoR, uKoL, uKoR, uhEff};
     in.v = redi::FaceIn{vPoL, vPoR, vKoL, vKoR, vhEff};
     double* trs[2] = {t_htr, s_htr};
-    rc = run_plain_phase_b(in, 2, trs, ws, st);
+    rc = run_phase_b<redi::PlainPrec>(in, 2, trs, ws, st);
     if (rc < 0) { report(rc, g_last_error); return; }
     cudaDeviceSynchronize();
 }

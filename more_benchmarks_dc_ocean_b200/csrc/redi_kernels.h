@@ -1,31 +1,70 @@
 // Internal launch interface of the Redi kernels (not part of the public C-ABI).
 #pragma once
 
+#include <cstdint>
 #include <cuda_runtime.h>
 
 #include "redi_device.cuh"
 
 namespace redi {
 
-constexpr int kNzMax = 128;       // layers per column supported by the FP64 kernels
+constexpr int kNzMax = 1024;      // layers per column accepted by the kernels
 constexpr int kMaxTracers = 64;   // tracers per fused launch (larger sets are split)
-constexpr int kCellGroup = 2;     // tracers accumulated together per cell thread
 
-struct FaceOut {
-    double* PoL;
-    double* PoR;
-    int* KoL;
-    int* KoR;
-    double* hEff;
+// ---------------------------------------------------------------------------
+// Precision policies.
+//
+// Plain: the reference's FP64 everywhere, coefficients in the reference layout
+// and types (bit-identical results).
+// Mixed: every quantity that feeds a discrete decision of the algorithm (the
+// sweep's density differences, interpolation denominators and positions; the
+// tracer values at neutral surfaces whose signs the down-gradient guard tests)
+// stays FP64 and is computed exactly as in the plain form; the PPM layer means
+// (redi_ppm_ave), the flux product and their storage are FP32; Ko is stored as
+// int16 and hEff as FP32; the flux divergence accumulates in FP64.
+// ---------------------------------------------------------------------------
+struct alignas(16) PpmLayerF {
+    float aL, dA, a6o3, B;
 };
 
-struct FaceIn {
-    const double* PoL;
-    const double* PoR;
-    const int* KoL;
-    const int* KoR;
-    const double* hEff;
+struct PlainPrec {
+    using Po = double;
+    using Ko = int;
+    using He = double;
+    using Ppm = PpmLayer;
+    using Flux = double;
+    static constexpr bool kMixed = false;
 };
+
+struct MixedPrec {
+    using Po = double;
+    using Ko = int16_t;
+    using He = float;
+    using Ppm = PpmLayerF;
+    using Flux = float;
+    static constexpr bool kMixed = true;
+};
+
+template <class P>
+struct FaceOutT {
+    typename P::Po* PoL;
+    typename P::Po* PoR;
+    typename P::Ko* KoL;
+    typename P::Ko* KoR;
+    typename P::He* hEff;
+};
+
+template <class P>
+struct FaceInT {
+    const typename P::Po* PoL;
+    const typename P::Po* PoR;
+    const typename P::Ko* KoL;
+    const typename P::Ko* KoR;
+    const typename P::He* hEff;
+};
+
+using FaceOut = FaceOutT<PlainPrec>;
+using FaceIn = FaceInT<PlainPrec>;
 
 struct ColumnStateArgs {
     int nx, ny, nz;
@@ -37,25 +76,30 @@ struct ColumnStateArgs {
     double* pint;    // [nz+1][column]
 };
 
-struct SweepArgs {
+template <class P>
+struct SweepArgsT {
     int nx, ny, nz;
     double rho0;
     const double* wet_u;
     const double* wet_v;
     const IfcState* ifc;
     const double* pint;
-    FaceOut u, v;
+    FaceOutT<P> u, v;
 };
+using SweepArgs = SweepArgsT<PlainPrec>;
 
-struct ReconArgs {
+template <class P>
+struct ReconArgsT {
     int nx, ny, nz, ntr;
     const double* h;
     const double* htr[kMaxTracers];
-    double* ti;      // [tracer][nz+1][column]
-    PpmLayer* ppm;   // [tracer][nz][column]
+    double* ti;               // [tracer][nz+1][column]
+    typename P::Ppm* ppm;     // [tracer][nz][column]
 };
+using ReconArgs = ReconArgsT<PlainPrec>;
 
-struct FaceFluxArgs {
+template <class P>
+struct FaceFluxArgsT {
     int nx, ny, nz, ntr;
     int nghost, nxp, nyp;
     int wall_w, wall_e, wall_s, wall_n;
@@ -67,38 +111,45 @@ struct FaceFluxArgs {
     const double* dx_cv;
     const double* idxCu;
     const double* idyCv;
-    FaceIn u, v;
-    const double* ti;       // [tracer][nz+1][column]
-    const PpmLayer* ppm;    // [tracer][nz][column]
-    double* Fu;             // [group tracer][ns-1][(nx+1)*ny]
-    double* Fv;             // [group tracer][ns-1][nx*(ny+1)]
+    FaceInT<P> u, v;
+    const double* ti;                 // [tracer][nz+1][column]
+    const typename P::Ppm* ppm;       // [tracer][nz][column]
+    typename P::Flux* Fu;             // [group tracer][ns-1][(nx+1)*ny]
+    typename P::Flux* Fv;             // [group tracer][ns-1][nx*(ny+1)]
 };
+using FaceFluxArgs = FaceFluxArgsT<PlainPrec>;
 
-struct CellGatherArgs {
+template <class P>
+struct CellGatherArgsT {
     int nx, ny, nz, ntr;
     int nghost, nxp, nyp;
     int wall_w, wall_e, wall_s, wall_n;
     const double* areaT;
-    FaceIn u, v;            // only KoL / KoR are read
-    const double* Fu;
-    const double* Fv;
+    FaceInT<P> u, v;                  // only KoL / KoR are read
+    const typename P::Flux* Fu;
+    const typename P::Flux* Fv;
     double* htr[kMaxTracers];
-    int* err;               // device error word (fluxes out of order), may be null
+    int* err;                         // device error word (fluxes out of order), may be null
 };
+using CellGatherArgs = CellGatherArgsT<PlainPrec>;
 
-// Scratch bytes each phase needs for an (nx, ny, nz) domain with ntr tracers.
-inline size_t plain_phase_a_scratch(int nx, int ny, int nz) {
+// Scratch bytes each phase needs for an (nx, ny, nz) domain.
+inline size_t phase_a_scratch(int nx, int ny, int nz) {
     const size_t nifc = (size_t)nx * ny * (nz + 1);
     return nifc * sizeof(IfcState) + nifc * sizeof(double);
 }
-inline size_t plain_recon_bytes(int nx, int ny, int nz, int ntr) {
+template <class P>
+inline size_t recon_bytes(int nx, int ny, int nz, int ntr) {
     const size_t ncol = (size_t)nx * ny;
-    return (size_t)ntr * ncol * ((nz + 1) * sizeof(double) + nz * sizeof(PpmLayer));
+    return (size_t)ntr * ncol * ((nz + 1) * sizeof(double) + nz * sizeof(typename P::Ppm));
 }
-inline size_t plain_flux_bytes(int nx, int ny, int nz, int group) {
+template <class P>
+inline size_t flux_bytes(int nx, int ny, int nz, int group) {
     const size_t faces = (size_t)(nx + 1) * ny + (size_t)nx * (ny + 1);
-    return (size_t)group * (size_t)(2 * nz + 1) * faces * sizeof(double);
+    return (size_t)group * (size_t)(2 * nz + 1) * faces * sizeof(typename P::Flux);
 }
+// Tracers per face-flux / gather launch for a set of ntr tracers.
+inline int tracer_group(int ntr) { return ntr >= 8 ? 8 : ntr >= 4 ? 4 : ntr >= 2 ? 2 : 1; }
 
 // Kernel identities for the launch counter and the optional event timing.
 enum KernelId : int {
@@ -121,7 +172,7 @@ enum KernelId : int {
 void launch_begin(int kid, cudaStream_t st);
 void launch_end(int kid, cudaStream_t st);
 
-// Launch shape of the FP64 cell update: a bx x by tile of columns per block
+// Launch shape of the cell gather: a bx x by tile of columns per block
 // (bx * by <= 128) and the vertical chunk (layers per pass, 4, 8 or 16).
 struct CellTuning {
     int bx, by, chunk;
@@ -129,8 +180,11 @@ struct CellTuning {
 CellTuning cell_tuning();
 void set_cell_tuning(const CellTuning& t);
 
-cudaError_t launch_plain_phase_a(const ColumnStateArgs& cs, const SweepArgs& sw, cudaStream_t st);
-cudaError_t launch_plain_phase_b(const ReconArgs& rc, const FaceFluxArgs& ff, const CellGatherArgs& cg,
-                                 cudaStream_t st);
+cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st);
+template <class P>
+cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st);
+template <class P>
+cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg,
+                           cudaStream_t st);
 
 }  // namespace redi

@@ -1,9 +1,11 @@
-// Plain FP64 Redi neutral-diffusion step for sm_100a.
+// Redi neutral-diffusion step for sm_100a: the plain FP64 form and the
+// mixed-precision form (precision policies in redi_kernels.h).
 //
 // Compiled with FMA contraction off (-fmad=false): every FP64 operation is the
-// reference's (redi/ocean_redi.F90), in the reference's order, so results are
-// bit-identical to the CPU oracle and to the reference's own CUDA ports built
-// the same way.
+// reference's (redi/ocean_redi.F90), in the reference's order, so the plain
+// form is bit-identical to the CPU oracle and to the reference's own CUDA ports
+// built the same way, and the mixed form takes every discrete decision exactly
+// as the plain form does.
 //
 // Decomposition (one column = all nz layers of one (i,j) T-cell):
 //
@@ -204,7 +206,8 @@ __device__ __forceinline__ IfcState sel(bool c, const IfcState& x, const IfcStat
 
 __device__ __forceinline__ IfcState win_own(const ColWin& w) { return sel(w.k == 1, w.a, w.b); }
 
-__global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
+template <class P>
+__global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgsT<P> a) {
     const int dir = blockIdx.y;  // 0: u-faces, 1: v-faces
     const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
     const size_t ld = (size_t)nx * ny;  // interface stride of the scratch
@@ -228,22 +231,25 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
         fo = i + nx * fj;
         fstride = (size_t)nx * (ny + 1);
     }
-    const FaceOut o = dir == 0 ? a.u : a.v;
-    double* __restrict__ PoL = o.PoL + fo;
-    double* __restrict__ PoR = o.PoR + fo;
-    int* __restrict__ KoL = o.KoL + fo;
-    int* __restrict__ KoR = o.KoR + fo;
-    double* __restrict__ hEff = o.hEff + fo;
+    using Po = typename P::Po;
+    using Ko = typename P::Ko;
+    using He = typename P::He;
+    const FaceOutT<P> o = dir == 0 ? a.u : a.v;
+    Po* __restrict__ PoL = o.PoL + fo;
+    Po* __restrict__ PoR = o.PoR + fo;
+    Ko* __restrict__ KoL = o.KoL + fo;
+    Ko* __restrict__ KoR = o.KoR + fo;
+    He* __restrict__ hEff = o.hEff + fo;
     const double wet = __ldg((dir == 0 ? a.wet_u : a.wet_v) + fo);
 
     if (!(wet > 0.0)) {  // ocean_redi.F90:722-730: inert coefficients
         for (int s = 0; s < ns; ++s) {
-            PoL[s * fstride] = 0.0;
-            PoR[s * fstride] = 0.0;
-            KoL[s * fstride] = 1;
-            KoR[s * fstride] = 1;
+            PoL[s * fstride] = Po(0);
+            PoR[s * fstride] = Po(0);
+            KoL[s * fstride] = Ko(1);
+            KoR[s * fstride] = Ko(1);
         }
-        for (int s = 0; s < ns - 1; ++s) hEff[s * fstride] = 0.0;
+        for (int s = 0; s < ns - 1; ++s) hEff[s * fstride] = He(0);
         return;
     }
 
@@ -345,16 +351,16 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
         lastK_right = kor;
         lastP_right = por;
         const size_t so = (size_t)(ks - 1) * fstride;
-        PoL[so] = pol;
-        PoR[so] = por;
-        KoL[so] = kol;
-        KoR[so] = kor;
+        PoL[so] = Po(pol);
+        PoR[so] = Po(por);
+        KoL[so] = Ko(kol);
+        KoR[so] = Ko(kor);
         if (ks > 1) {  // harmonic-mean effective thickness (:452-462), Pa -> m (:688-691)
             const double hL = absL - absL_prev;
             const double hR = absR - absR_prev;
             double he = 0.0;
             if (hL + hR > 0.0) he = 2.0 * hL * hR / (hL + hR);
-            hEff[so - fstride] = he * pa_to_h;
+            hEff[so - fstride] = He(he * pa_to_h);
         }
         absL_prev = absL;
         absR_prev = absR;
@@ -367,8 +373,21 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgs a) {
 // interface values Tint and the nz prepared PPM layers in [layer][column]
 // order, so that threads of neighbouring columns touch neighbouring addresses.
 // ---------------------------------------------------------------------------
-template <int NT>
-__global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
+template <class P>
+__device__ __forceinline__ void store_ppm(typename P::Ppm* p, const PpmLayer& q);
+template <>
+__device__ __forceinline__ void store_ppm<PlainPrec>(PpmLayer* p, const PpmLayer& q) {
+    double2* d = reinterpret_cast<double2*>(p);
+    d[0] = make_double2(q.aL, q.dA);
+    d[1] = make_double2(q.a6o3, q.B);
+}
+template <>
+__device__ __forceinline__ void store_ppm<MixedPrec>(PpmLayerF* p, const PpmLayer& q) {
+    *reinterpret_cast<float4*>(p) = make_float4((float)q.aL, (float)q.dA, (float)q.a6o3, (float)q.B);
+}
+
+template <int NT, class P>
+__global__ void __launch_bounds__(128) k_tracer_recon(ReconArgsT<P> a) {
     const int ncol = a.nx * a.ny;
     const int ngroups = (a.ntr + NT - 1) / NT;
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -381,7 +400,7 @@ __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
     const double* __restrict__ h = a.h + col;
     const double* htr[NT];
     double* ti[NT];
-    PpmLayer* ppm[NT];
+    typename P::Ppm* ppm[NT];
 #pragma unroll
     for (int n = 0; n < NT; ++n) {
         const int tr = tr0 + (n < nt ? n : 0);
@@ -408,10 +427,7 @@ __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
                     double alk = e_prev[n], ark = e[n];
                     const double tlk = s_above[n];
                     ppm_limit(alk, ark, tlk);
-                    const PpmLayer q = make_ppm_layer(alk, ark, tlk);
-                    double2* p = reinterpret_cast<double2*>(ppm[n] + (size_t)(t - 2) * ncol);
-                    p[0] = make_double2(q.aL, q.dA);
-                    p[1] = make_double2(q.a6o3, q.B);
+                    store_ppm<P>(ppm[n] + (size_t)(t - 2) * ncol, make_ppm_layer(alk, ark, tlk));
                 }
             }
             e_prev[n] = e[n];
@@ -433,8 +449,43 @@ __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgs a) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double interp(double P, double a, double b) { return (1.0 - P) * a + P * b; }
 
-template <int NT>
-__global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgs a, int tr0) {
+// Layer mean of the PPM parabola and the flux product, per precision.
+template <class P>
+struct FluxOps;
+
+template <>
+struct FluxOps<PlainPrec> {
+    using Mean = double;
+    __device__ static __forceinline__ double mean(double xL, double xR, const PpmLayer* p) {
+        return ppm_ave(xL, xR, load_ppm(p));
+    }
+    __device__ static __forceinline__ double flux(double dT, double he, double coef) { return dT * he * coef; }
+};
+
+template <>
+struct FluxOps<MixedPrec> {
+    using Mean = float;
+    // redi_ppm_ave in FP32; the branch (a discrete decision) is taken on the
+    // FP64 positions exactly as in the plain form.
+    __device__ static __forceinline__ float mean(double xL, double xR, const PpmLayerF* p) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(p));  // aL, dA, a6o3, B
+        const float xl = (float)xL, xr = (float)xR;
+        const double dx = xR - xL;
+        if (dx > 0.0 && dx <= 1.0) {
+            const float xave = 0.5f * (xr + xl);
+            return (q.x + xave * q.w) - q.z * (xr * xr + xr * xl + xl * xl);
+        }
+        const float a6 = 3.0f * q.z;
+        return q.x + q.y * xr + a6 * xr * (1.0f - xr);
+    }
+    __device__ static __forceinline__ float flux(double dT, float he, double coef) {
+        return (float)dT * he * (float)coef;
+    }
+};
+
+template <int NT, class P>
+__global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0) {
+    using Ops = FluxOps<P>;
     const int dir = blockIdx.y;  // 0: u-faces, 1: v-faces
     const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
     const size_t ncol = (size_t)nx * ny;
@@ -460,12 +511,12 @@ __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgs a, int tr0) {
         fo = i + nx * fj;
         fstride = (size_t)nx * (ny + 1);
     }
-    const FaceIn& c = dir == 0 ? a.u : a.v;
-    const double* __restrict__ hEff = c.hEff + fo;
-    const double* __restrict__ PoL = c.PoL + fo;
-    const double* __restrict__ PoR = c.PoR + fo;
-    const int* __restrict__ KoL = c.KoL + fo;
-    const int* __restrict__ KoR = c.KoR + fo;
+    const FaceInT<P>& c = dir == 0 ? a.u : a.v;
+    const typename P::He* __restrict__ hEff = c.hEff + fo;
+    const typename P::Po* __restrict__ PoL = c.PoL + fo;
+    const typename P::Po* __restrict__ PoR = c.PoR + fo;
+    const typename P::Ko* __restrict__ KoL = c.KoL + fo;
+    const typename P::Ko* __restrict__ KoR = c.KoR + fo;
     const double* kh = dir == 0 ? a.khtr_u : a.khtr_v;
     const double khv = kh ? __ldg(kh + fo) : a.khtr;
     // ((dt*khtr)*dy)*idx, ocean_redi.F90:1156/1168
@@ -474,9 +525,9 @@ __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgs a, int tr0) {
     const int nt = min(NT, a.ntr - tr0);
     const double* tiL[NT];
     const double* tiR[NT];
-    const PpmLayer* ppL[NT];
-    const PpmLayer* ppR[NT];
-    double* Fo[NT];
+    const typename P::Ppm* ppL[NT];
+    const typename P::Ppm* ppR[NT];
+    typename P::Flux* Fo[NT];
 #pragma unroll
     for (int n = 0; n < NT; ++n) {
         const int tr = tr0 + (n < nt ? n : 0);
@@ -487,55 +538,72 @@ __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgs a, int tr0) {
         Fo[n] = (dir == 0 ? a.Fu : a.Fv) + (size_t)(tr - tr0) * (size_t)(ns - 1) * fstride + fo;
     }
 
-    int cached = -1;  // surface whose tracer values are held in tl/tr
-    int kl_t = 1, kr_t = 1;
-    double pl_t = 0.0, pr_t = 0.0;
+    // Register rotation: while sublayer s is evaluated, hEff(s+1) and the
+    // bottom surface of s+1 (surface s+2) are already being fetched. The top
+    // surface of s is always the bottom surface of s-1.
+    using He = typename P::He;
+    bool have_t = false;  // tl/tr hold the tracer values at the top surface
+    int kl_t = min(max((int)__ldg(KoL), 1), nz), kr_t = min(max((int)__ldg(KoR), 1), nz);
+    double pl_t = __ldg(PoL), pr_t = __ldg(PoR);
+    He he_c = __ldg(hEff);
+    int klr_c = __ldg(KoL + fstride), krr_c = __ldg(KoR + fstride);
+    double pl_c = __ldg(PoL + fstride), pr_c = __ldg(PoR + fstride);
     double tl[NT], tr[NT];
     for (int s = 0; s < ns - 1; ++s) {
         const size_t s0 = (size_t)s * fstride;
-        const double he = __ldg(hEff + s0);
-        if (he == 0.0) {
+        He he_n = He(0);
+        int klr_n = 1, krr_n = 1;
+        double pl_n = 0.0, pr_n = 0.0;
+        if (s + 1 < ns - 1) {
+            const size_t s2 = s0 + 2 * fstride;
+            he_n = __ldg(hEff + s0 + fstride);
+            klr_n = __ldg(KoL + s2);
+            krr_n = __ldg(KoR + s2);
+            pl_n = __ldg(PoL + s2);
+            pr_n = __ldg(PoR + s2);
+        }
+        const int kl_b = min(max(klr_c, 1), nz);
+        const int kr_b = min(max(krr_c, 1), nz);
+        const double pl_b = pl_c, pr_b = pr_c;
+        if (he_c == He(0)) {
 #pragma unroll
             for (int n = 0; n < NT; ++n)
-                if (n < nt) Fo[n][s0] = 0.0;
-            continue;
-        }
-        if (cached != s) {
-            kl_t = min(max(__ldg(KoL + s0), 1), nz);
-            kr_t = min(max(__ldg(KoR + s0), 1), nz);
-            pl_t = __ldg(PoL + s0);
-            pr_t = __ldg(PoR + s0);
+                if (n < nt) Fo[n][s0] = typename P::Flux(0);
+            have_t = false;
+        } else {
+            if (!have_t) {
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    tl[n] = interp(pl_t, __ldg(tiL[n] + (size_t)(kl_t - 1) * ncol), __ldg(tiL[n] + (size_t)kl_t * ncol));
+                    tr[n] = interp(pr_t, __ldg(tiR[n] + (size_t)(kr_t - 1) * ncol), __ldg(tiR[n] + (size_t)kr_t * ncol));
+                }
+            }
+            const double xRl = pl_b + (double)(kl_b - kl_t);
+            const double xRr = pr_b + (double)(kr_b - kr_t);
 #pragma unroll
             for (int n = 0; n < NT; ++n) {
-                tl[n] = interp(pl_t, __ldg(tiL[n] + (size_t)(kl_t - 1) * ncol), __ldg(tiL[n] + (size_t)kl_t * ncol));
-                tr[n] = interp(pr_t, __ldg(tiR[n] + (size_t)(kr_t - 1) * ncol), __ldg(tiR[n] + (size_t)kr_t * ncol));
+                const double bl = interp(pl_b, __ldg(tiL[n] + (size_t)(kl_b - 1) * ncol), __ldg(tiL[n] + (size_t)kl_b * ncol));
+                const double br = interp(pr_b, __ldg(tiR[n] + (size_t)(kr_b - 1) * ncol), __ldg(tiR[n] + (size_t)kr_b * ncol));
+                if (n < nt) {
+                    const typename Ops::Mean tlay = Ops::mean(pl_t, xRl, ppL[n] + (size_t)(kl_t - 1) * ncol);
+                    const typename Ops::Mean trlay = Ops::mean(pr_t, xRr, ppR[n] + (size_t)(kr_t - 1) * ncol);
+                    const double dT = guarded_dT(tr[n] - tl[n], br - bl, (double)(trlay - tlay));
+                    Fo[n][s0] = Ops::flux(dT, he_c, coef);
+                }
+                tl[n] = bl;
+                tr[n] = br;
             }
+            have_t = true;
         }
-        const size_t s1 = s0 + fstride;
-        const int kl_b = min(max(__ldg(KoL + s1), 1), nz);
-        const int kr_b = min(max(__ldg(KoR + s1), 1), nz);
-        const double pl_b = __ldg(PoL + s1);
-        const double pr_b = __ldg(PoR + s1);
-        const double xRl = pl_b + (double)(kl_b - kl_t);
-        const double xRr = pr_b + (double)(kr_b - kr_t);
-#pragma unroll
-        for (int n = 0; n < NT; ++n) {
-            const double bl = interp(pl_b, __ldg(tiL[n] + (size_t)(kl_b - 1) * ncol), __ldg(tiL[n] + (size_t)kl_b * ncol));
-            const double br = interp(pr_b, __ldg(tiR[n] + (size_t)(kr_b - 1) * ncol), __ldg(tiR[n] + (size_t)kr_b * ncol));
-            if (n < nt) {
-                const double tlay = ppm_ave(pl_t, xRl, load_ppm(ppL[n] + (size_t)(kl_t - 1) * ncol));
-                const double trlay = ppm_ave(pr_t, xRr, load_ppm(ppR[n] + (size_t)(kr_t - 1) * ncol));
-                const double dT = guarded_dT(tr[n] - tl[n], br - bl, trlay - tlay);
-                Fo[n][s0] = dT * he * coef;
-            }
-            tl[n] = bl;
-            tr[n] = br;
-        }
-        cached = s + 1;
         kl_t = kl_b;
         kr_t = kr_b;
         pl_t = pl_b;
         pr_t = pr_b;
+        he_c = he_n;
+        klr_c = klr_n;
+        krr_c = krr_n;
+        pl_c = pl_n;
+        pr_c = pr_n;
     }
 }
 
@@ -560,34 +628,58 @@ __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgs a, int tr0) {
 // possible for sweep-produced coefficients) is counted in the device error
 // word and skipped.
 // ---------------------------------------------------------------------------
-template <int NT, int CH>
-__device__ __forceinline__ void gather_run(const double* const (&F)[NT], const int* __restrict__ KoS, size_t stride,
-                                           bool left, int ns, int& ptr, int k0, int k1, double (&dTr)[NT][CH],
-                                           int& bad) {
+template <int NT, int CH, class P>
+__device__ __forceinline__ void gather_run(const typename P::Flux* const (&F)[NT],
+                                           const typename P::Ko* __restrict__ KoS, size_t stride, bool left, int ns,
+                                           int& ptr, int k0, int k1, double (&dTr)[NT][CH], int& bad) {
+    // Sublayers are fetched U at a time (independent loads in flight), then
+    // consumed in order until the first one beyond the chunk.
+    constexpr int U = 4;
     int cur = -1;
     double acc[NT];
     int s = ptr;
-    for (; s < ns - 1; ++s) {
-        const size_t so = (size_t)s * stride;
-        const int k = __ldg(KoS + so);
-        if (k >= k1) break;
-        if (k < k0) {
-            ++bad;
-            continue;
-        }
-        const int slot = k - k0;
-        if (slot != cur) {
+    bool done = false;
+    while (!done && s < ns - 1) {
+        int kk[U];
+        double ff[U][NT];
 #pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                if (cur >= 0) dTr[n][cur] = acc[n];
-                acc[n] = dTr[n][slot];
+        for (int u = 0; u < U; ++u) {
+            const int su = s + u;
+            if (su < ns - 1) {
+                const size_t so = (size_t)su * stride;
+                kk[u] = (int)__ldg(KoS + so);
+#pragma unroll
+                for (int n = 0; n < NT; ++n) ff[u][n] = (double)__ldg(F[n] + so);
+            } else {
+                kk[u] = 0x7fffffff;
+#pragma unroll
+                for (int n = 0; n < NT; ++n) ff[u][n] = 0.0;
             }
-            cur = slot;
         }
 #pragma unroll
-        for (int n = 0; n < NT; ++n) {
-            const double flx = __ldg(F[n] + so);
-            acc[n] = left ? acc[n] + flx : acc[n] - flx;
+        for (int u = 0; u < U; ++u) {
+            if (done) break;
+            const int k = kk[u];
+            if (k >= k1) {  // also the end of the face (s >= ns-1)
+                done = true;
+                break;
+            }
+            ++s;
+            if (k < k0) {
+                ++bad;
+                continue;
+            }
+            const int slot = k - k0;
+            if (slot != cur) {
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    if (cur >= 0) dTr[n][cur] = acc[n];
+                    acc[n] = dTr[n][slot];
+                }
+                cur = slot;
+            }
+#pragma unroll
+            for (int n = 0; n < NT; ++n) acc[n] = left ? acc[n] + ff[u][n] : acc[n] - ff[u][n];
         }
     }
     ptr = s;
@@ -597,8 +689,8 @@ __device__ __forceinline__ void gather_run(const double* const (&F)[NT], const i
     }
 }
 
-template <int NT, int CH>
-__global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgs a, int tr0) {
+template <int NT, int CH, class P>
+__global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgsT<P> a, int tr0) {
     const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -632,12 +724,12 @@ __global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgs a, int tr0) 
             if (!on[f]) continue;
             const bool u = f < 2, left = (f & 1) != 0;
             const size_t stride = u ? ustride : vstride;
-            const double* F[NT];
+            const typename P::Flux* F[NT];
 #pragma unroll
             for (int n = 0; n < NT; ++n)
                 F[n] = (u ? a.Fu : a.Fv) + (size_t)(n < nt ? n : 0) * (size_t)(ns - 1) * stride + fo[f];
-            const FaceIn& c = u ? a.u : a.v;
-            gather_run<NT, CH>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1, dTr, bad);
+            const FaceInT<P>& c = u ? a.u : a.v;
+            gather_run<NT, CH, P>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1, dTr, bad);
         }
         // Layers k0..k1-1 are complete: hTr(knat) += dTr(knat) * (1/areaT), knat = nz + 1 - k.
 #pragma unroll
@@ -665,51 +757,79 @@ __global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgs a, int tr0) 
 // ---------------------------------------------------------------------------
 // Host launchers (stream-ordered, no synchronisation).
 // ---------------------------------------------------------------------------
-cudaError_t launch_plain_phase_a(const ColumnStateArgs& cs, const SweepArgs& sw, cudaStream_t st) {
+cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st) {
     const int ncol = cs.nx * cs.ny;
     launch_begin(K_COLUMN_STATE, st);
     plain::k_column_state<<<(ncol + 127) / 128, 128, 0, st>>>(cs);
     launch_end(K_COLUMN_STATE, st);
+    return cudaGetLastError();
+}
+
+template <class P>
+cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st) {
     const int nface = max((sw.nx - 1) * sw.ny, sw.nx * (sw.ny - 1));
     if (nface > 0) {
+        const int kid = P::kMixed ? K_MIXED_SWEEP : K_NEUTRAL_SWEEP;
         dim3 grid((nface + 127) / 128, 2);
-        launch_begin(K_NEUTRAL_SWEEP, st);
-        plain::k_neutral_sweep<<<grid, 128, 0, st>>>(sw);
-        launch_end(K_NEUTRAL_SWEEP, st);
+        launch_begin(kid, st);
+        plain::k_neutral_sweep<P><<<grid, 128, 0, st>>>(sw);
+        launch_end(kid, st);
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_plain_phase_b(const ReconArgs& rc, const FaceFluxArgs& ff, const CellGatherArgs& cg,
-                                 cudaStream_t st) {
+template <int NT, class P>
+static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg, int tr0, int nface,
+                               const CellTuning& tune, cudaStream_t st) {
+    const dim3 block(tune.bx, tune.by);
+    const dim3 cgrid((cg.nx + tune.bx - 1) / tune.bx, (cg.ny + tune.by - 1) / tune.by);
+    if (nface > 0) {
+        const int kid = P::kMixed ? K_MIXED_FLUX : K_FACE_FLUX;
+        launch_begin(kid, st);
+        plain::k_face_flux<NT, P><<<dim3((nface + 127) / 128, 2), 128, 0, st>>>(ff, tr0);
+        launch_end(kid, st);
+    }
+    launch_begin(K_CELL_UPDATE, st);
+    switch (tune.chunk) {
+        case 4: plain::k_cell_gather<NT, 4, P><<<cgrid, block, 0, st>>>(cg, tr0); break;
+        case 16: plain::k_cell_gather<NT, 16, P><<<cgrid, block, 0, st>>>(cg, tr0); break;
+        default: plain::k_cell_gather<NT, 8, P><<<cgrid, block, 0, st>>>(cg, tr0); break;
+    }
+    launch_end(K_CELL_UPDATE, st);
+}
+
+template <class P>
+cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg,
+                           cudaStream_t st) {
     const int ncol = rc.nx * rc.ny;
     // Reconstruct in groups of two tracers (register window of 2 scalars).
     {
         const int ngroups = (rc.ntr + 1) / 2;
         const long long n = (long long)ncol * ngroups;
-        launch_begin(K_TRACER_RECON, st);
-        plain::k_tracer_recon<2><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc);
-        launch_end(K_TRACER_RECON, st);
+        const int kid = P::kMixed ? K_MIXED_RECON : K_TRACER_RECON;
+        launch_begin(kid, st);
+        plain::k_tracer_recon<2, P><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc);
+        launch_end(kid, st);
     }
     const CellTuning tune = cell_tuning();
-    const dim3 block(tune.bx, tune.by);
-    const dim3 cgrid((cg.nx + tune.bx - 1) / tune.bx, (cg.ny + tune.by - 1) / tune.by);
     const int nface = max((ff.nx - 1) * ff.ny, ff.nx * (ff.ny - 1));
-    for (int tr0 = 0; tr0 < ff.ntr; tr0 += kCellGroup) {
-        if (nface > 0) {
-            launch_begin(K_FACE_FLUX, st);
-            plain::k_face_flux<kCellGroup><<<dim3((nface + 127) / 128, 2), 128, 0, st>>>(ff, tr0);
-            launch_end(K_FACE_FLUX, st);
+    const int group = tracer_group(ff.ntr);
+    for (int tr0 = 0; tr0 < ff.ntr; tr0 += group) {
+        switch (group) {
+            case 8: launch_flux_gather<8, P>(ff, cg, tr0, nface, tune, st); break;
+            case 4: launch_flux_gather<4, P>(ff, cg, tr0, nface, tune, st); break;
+            case 2: launch_flux_gather<2, P>(ff, cg, tr0, nface, tune, st); break;
+            default: launch_flux_gather<1, P>(ff, cg, tr0, nface, tune, st); break;
         }
-        launch_begin(K_CELL_UPDATE, st);
-        switch (tune.chunk) {
-            case 4: plain::k_cell_gather<kCellGroup, 4><<<cgrid, block, 0, st>>>(cg, tr0); break;
-            case 16: plain::k_cell_gather<kCellGroup, 16><<<cgrid, block, 0, st>>>(cg, tr0); break;
-            default: plain::k_cell_gather<kCellGroup, 8><<<cgrid, block, 0, st>>>(cg, tr0); break;
-        }
-        launch_end(K_CELL_UPDATE, st);
     }
     return cudaGetLastError();
 }
+
+template cudaError_t launch_sweep<PlainPrec>(const SweepArgsT<PlainPrec>&, cudaStream_t);
+template cudaError_t launch_sweep<MixedPrec>(const SweepArgsT<MixedPrec>&, cudaStream_t);
+template cudaError_t launch_phase_b<PlainPrec>(const ReconArgsT<PlainPrec>&, const FaceFluxArgsT<PlainPrec>&,
+                                               const CellGatherArgsT<PlainPrec>&, cudaStream_t);
+template cudaError_t launch_phase_b<MixedPrec>(const ReconArgsT<MixedPrec>&, const FaceFluxArgsT<MixedPrec>&,
+                                               const CellGatherArgsT<MixedPrec>&, cudaStream_t);
 
 }  // namespace redi
