@@ -206,6 +206,32 @@ REDI_B200_API void redi_cuda_launch_(const int* nx, const int* ny, const int* nz
                        double* khtr_v, const double* dy_cu, const double* dx_cv, const double* idxCu,
                        const double* idyCv, const double* areaT, double* tr_snap);
 
+/* The reference-compatible step without any device allocation. No counterpart
+ * in the reference. For callers that must not call cudaMalloc/cudaFree while
+ * stepping: those calls can synchronise the whole device, cannot run while a
+ * stream is being captured, and some host models hand out all device memory
+ * from their own pool. Arguments and results are those of redi_opt_launch (all
+ * arrays device pointers, scalars by reference; tr_snap is not written), plus
+ * the stream to run on (NULL: legacy default stream); the call is
+ * stream-ordered and does not synchronise.
+ * Scratch comes from one 64 MiB array inside the library, held on every GPU
+ * that loads the library until exit, and shared by all calls: calls that
+ * overlap on the GPU race on it, so issue them in stream order. Its device
+ * address is resolved by the first call on each device: make that call before
+ * any stream capture. A domain whose scratch exceeds 64 MiB (about 18 000
+ * columns at nz = 25, 6 000 at nz = 75) is refused with
+ * REDI_B200_E_UNSUPPORTED; the message (redi_b200_last_error) gives the
+ * limit. Returns REDI_B200_OK or a negative status. */
+REDI_B200_API int redi_b200_opt_launch_noalloc(
+    const int* nx, const int* ny, const int* nz, const int* ns, const double* dt, const int* nghost, const int* nxp,
+    const int* nyp, const int* ww, const int* we, const int* wsz, const int* wn, const double* rho0,
+    const double* T_ref, const double* S_ref, const double* alpha_T, const double* beta_S, const double* h_layer,
+    double* t_htr, double* s_htr, const double* wet_u, const double* wet_v, double* uPoL, double* uPoR, int* uKoL,
+    int* uKoR, double* uhEff, double* vPoL, double* vPoR, int* vKoL, int* vKoR, double* vhEff,
+    const double* khtr_u_ext, const double* khtr_v_ext, double* khtr_u, double* khtr_v, const double* dy_cu,
+    const double* dx_cv, const double* idxCu, const double* idyCv, const double* areaT, double* tr_snap,
+    void* stream);
+
 #ifdef __cplusplus
 }
 #endif

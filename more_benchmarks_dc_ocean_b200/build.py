@@ -25,6 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hi
 SOURCES = [
     ("redi_plain.cu", ["-fmad=false"]),
     ("redi_capi.cu", []),
+    ("redi_noalloc.cu", []),
 ]
 
 

@@ -204,6 +204,8 @@ Profiler g_prof;
 }  // namespace
 
 namespace redi {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 static CellTuning g_cell_tuning{32, 4, 8};
 CellTuning cell_tuning() { return g_cell_tuning; }
 void set_cell_tuning(const CellTuning& t) { g_cell_tuning = t; }

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "redi_device.cuh"
@@ -165,6 +166,9 @@ enum KernelId : int {
     K_AUX = 9,
     K_NUM = 10
 };
+
+// Sets the message redi_b200_last_error() returns on the calling thread.
+void set_last_error(const std::string& msg);
 
 // Launch bracketing: counts every kernel launch of the library and, while
 // timing is switched on (redi_b200_profile_begin), records a CUDA event pair
