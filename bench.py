@@ -1,7 +1,7 @@
 """Benchmark of the Redi neutral-diffusion step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--config config1|config3|config0] [--precision fp64|mixed]
+                    [--config config1|config3|config0|config4] [--precision fp64|mixed]
 
 One step = redi_calc_coeffs + redi_apply_flux over every tracer of the domain.
 Metric: tracer-cell updates/s = N_tracers * nx_phys * ny_phys * nz
@@ -233,7 +233,14 @@ def cpu_sample(p, target_s: float, nsteps: int = 1, warmup: int = 0):
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    p = _problem(args.config, args.grid)
+    if args.config == "config4":  # the largest domain of the batch stands for the whole set
+        from more_benchmarks_dc_ocean_b200 import inputs
+
+        shapes = inputs.config4_shapes()
+        d = max(range(len(shapes)), key=lambda i: shapes[i][0] * shapes[i][1] * shapes[i][2])
+        p = inputs.config4_domain(20261203, d, shapes[d])
+    else:
+        p = _problem(args.config, args.grid)
     budget = 150.0
     per_step = max(2.0, budget / max(1, args.steps + args.warmup))
     upd, info = cpu_sample(p, per_step, nsteps=args.steps, warmup=args.warmup)
@@ -399,6 +406,248 @@ def run_b200(args, rank, world, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Uneven-domain batch (config4): one persistent kernel over a tile-work queue
+# ---------------------------------------------------------------------------
+def _domains_config_block(ps, args, world, prec_name):
+    shapes = [(p.nx_phys, p.ny_phys, p.nz) for p in ps]
+    return {
+        "workload": f"config4: {len(ps)} uneven regional domains (nx, ny log-uniform in [64, 512], nz in "
+                    f"{{25, 50, 75}}), {ps[0].ntr} tracers each, {prec_name} Redi step, one persistent kernel "
+                    "replayed from a CUDA graph" + (f", {world} ranks x {len(ps)} domains" if world > 1 else ""),
+        "domains": len(ps), "tracers": ps[0].ntr, "cells": int(sum(a * b * c for a, b, c in shapes)),
+        "nx_range": [min(a for a, _, _ in shapes), max(a for a, _, _ in shapes)],
+        "ny_range": [min(b for _, b, _ in shapes), max(b for _, b, _ in shapes)],
+        "nz_set": sorted({c for _, _, c in shapes}), "precision": args.precision,
+        "l2": "inputs larger than L2 (126 MB), no flush",
+        "parallelism": f"dp{world}" if world > 1 else "1 GPU",
+    }
+
+
+def run_domains(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+
+    from more_benchmarks_dc_ocean_b200 import autotune, inputs
+    from more_benchmarks_dc_ocean_b200 import ocean_redi as R
+
+    # Inputs are generated before the first GPU call (the pool is spawned).
+    workers = max(1, min(len(os.sched_getaffinity(0)), 16))
+    t_gen = time.perf_counter()
+    ps = inputs.config4(seed=20261203 + 1000 * rank, workers=workers)
+    t_gen = time.perf_counter() - t_gen
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    dps = [R.to_device(p, dev) for p in ps]
+    st = torch.cuda.current_stream()
+    L = R.lib()
+    L.redi_b200_launch_count.restype = C.c_ulonglong
+    L.redi_b200_launch_count.argtypes = [C.c_int]
+    prec_main = R.FP64 if args.precision == "fp64" else R.MIXED
+
+    def reset_inputs():
+        for p, dp in zip(ps, dps):
+            dp.ms.h_layer.copy_(torch.from_numpy(p.h))
+            for d, h in zip(dp.ms.tracers, p.tracers):
+                d.copy_(torch.from_numpy(h))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(batch, steps):
+        barrier()
+        torch.cuda.synchronize()
+        L.redi_b200_profile_begin()
+        n0 = L.redi_b200_launch_count(-1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        batch.step(steps, st)
+        e1.record(st)
+        torch.cuda.synchronize()
+        n1 = L.redi_b200_launch_count(-1)
+        kt = (C.c_double * NKERN)()
+        kc = (C.c_ulonglong * NKERN)()
+        L.redi_b200_profile_end(kt, kc, NKERN)
+        barrier()
+        return e0.elapsed_time(e1) / steps, kt, kc, int(n1 - n0)
+
+    results = {}
+    fp64_after_one = None
+    for prec in ([R.FP64, R.MIXED] if prec_main == R.FP64 else [R.MIXED, R.FP64]):
+        name = "fp64" if prec == R.FP64 else "mixed"
+        reset_inputs()
+        batch = R.RediBatch(dps, precision=prec)
+        # One step from the initial state: FP64 is kept as the reference (bit-identical to the
+        # oracle), the mixed result is compared with it domain by domain.
+        batch.step(1, st)
+        torch.cuda.synchronize()
+        stat = batch.status()
+        if prec == R.FP64:
+            fp64_after_one = [[t.clone() for t in dp.ms.tracers] for dp in dps]
+            err = None
+        else:
+            err = []
+            if fp64_after_one is None:  # mixed ran first: make the FP64 reference now
+                keep = [[t.clone() for t in dp.ms.tracers] for dp in dps]
+                reset_inputs()
+                ref_b = R.RediBatch(dps, precision=R.FP64)
+                ref_b.step(1, st)
+                torch.cuda.synchronize()
+                fp64_after_one = [[t.clone() for t in dp.ms.tracers] for dp in dps]
+                ref_b.destroy()
+                for dp, k in zip(dps, keep):
+                    for d, t in zip(dp.ms.tracers, k):
+                        d.copy_(t)
+                del keep
+            for d, (dp, ref) in enumerate(zip(dps, fp64_after_one)):
+                worst = 0.0
+                for t, r in zip(dp.ms.tracers, ref):
+                    worst = max(worst, float((t - r).abs().max()) / max(float(r.abs().max()), 1e-300))
+                err.append(worst)
+        tuning = None
+        if not args.no_tune:
+            tuning = autotune.tune_batch(batch, reps=2, stream=st)
+            if dist is not None:
+                t = torch.tensor(list(tuning["best"]), dtype=torch.int64, device=dev)
+                dist.broadcast(t, 0)
+                best = tuple(int(v) for v in t.tolist())
+                batch.set_tuning(best[:2], best[2], best[3])
+                tuning["best"] = best
+        batch.step(args.warmup, st)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(_uuid(local_rank)) if prec == prec_main else None
+        if clocks:
+            clocks.start()
+        ms, kt, kc, launches = timed(batch, args.steps)
+        clk = clocks.stop() if clocks else None
+        batch.set_accounting(True)  # one more (untimed) step with per-stage accounting
+        batch.step(1, st)
+        stages = batch.stage_times()
+        batch.set_accounting(False)
+        ms_all = _max_over_ranks(ms, dist, dev)
+        k = 8  # k_domain_persistent
+        bytes_launch = float(sum(boundary_bytes(p, name) for p in ps))
+        t_launch = kt[k] / max(1, kc[k]) * 1e-3
+        results[name] = {
+            "value": batch.updates * world / (ms_all * 1e-3), "ms_per_step": ms_all, "kernel_ms": kt[k] / max(1, kc[k]),
+            "launches": launches, "bytes": bytes_launch, "achieved_gbs": bytes_launch / t_launch / 1e9,
+            "status": stat, "clocks": clk, "updates": batch.updates, "items": batch.items,
+            "stage_accounting_ms_summed_over_blocks": {k: {kk: round(vv, 3) if isinstance(vv, float) else vv
+                                                           for kk, vv in v.items()} for k, v in stages.items()},
+            "tuning": {"gather_tile": list(tuning["best"][:2]), "vertical_chunk": tuning["best"][2],
+                       "occupancy": tuning["best"][3],
+                       "grid_blocks": batch.get_tuning()["grid"], "candidates_ms": tuning["ms"]} if tuning else
+            batch.get_tuning(),
+            "per_domain_max_rel_err_vs_fp64_1step": ({"max": max(err), "median": statistics.median(err),
+                                                      "all": [float(f"{e:.3e}") for e in err]} if err else None),
+        }
+        if prec == prec_main:
+            results[name]["e2e"] = None if args.no_e2e else _domains_e2e(args, ps, dps, batch, st, dist, dev, world)
+        batch.destroy()
+        torch.cuda.synchronize()
+    del fp64_after_one
+
+    # Baseline on the same GPU: every domain stepped through the handle API, one after another.
+    reset_inputs()
+    handles = [R.make_redi(dp, prec_main) for dp in dps]
+    for dp, h in zip(dps, handles):
+        R.step(dp, h, args.warmup, st)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = L.redi_b200_launch_count(-1)
+    L.redi_b200_profile_begin()
+    e0.record(st)
+    for _ in range(args.steps):
+        for dp, h in zip(dps, handles):
+            R.step(dp, h, 1, st)
+    e1.record(st)
+    torch.cuda.synchronize()
+    skt = (C.c_double * NKERN)()
+    skc = (C.c_ulonglong * NKERN)()
+    L.redi_b200_profile_end(skt, skc, NKERN)
+    seq_kernels = {KERNEL_NAMES[k]: round(skt[k] / args.steps, 3) for k in range(NKERN) if skc[k]}
+    seq_launches = int(L.redi_b200_launch_count(-1) - n0) // args.steps
+    seq_ms = _max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
+    for h in handles:
+        h.destroy()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        big = max(ps, key=lambda p: p.ncell)
+        upd, info = cpu_sample(big, args.cpu_seconds)
+        cpu = {"value": upd, "unit": UNIT, "cores": info["cores"], "kind": "port", "sample": info["sample"]}
+
+    main = results[args.precision]
+    peak, peak_kind = _peaks()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": main["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32", "data": "synthetic",
+            "config": _domains_config_block(ps, args, world, "plain FP64" if args.precision == "fp64" else "mixed"),
+            "roofline": {"bound": "hbm", "kernel": "k_domain_persistent", "achieved": main["achieved_gbs"],
+                         "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": main["achieved_gbs"] / peak,
+                         "traffic": None, "algorithmic_bytes_per_launch": main["bytes"]},
+            "side_by_side": {k: {kk: vv for kk, vv in v.items() if kk not in ("clocks", "e2e")}
+                             for k, v in results.items()},
+            "per_domain_launch_baseline": {"value": main["updates"] * world / (seq_ms * 1e-3), "ms_per_step": seq_ms,
+                                           "launches_per_step": seq_launches, "kernel_ms_per_step": seq_kernels,
+                                           "path": "handle API, one domain after another"},
+            "cpu_baseline": cpu,
+            "e2e": main["e2e"],
+            "clocks": main["clocks"],
+            "gpu_launches": main["launches"],
+            "input_generation_s": round(t_gen, 1),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _domains_e2e(args, ps, dps, batch, st, dist, dev, world):
+    import torch
+
+    host = [(torch.from_numpy(p.h).pin_memory(), [torch.from_numpy(t).pin_memory() for t in p.tracers]) for p in ps]
+
+    def e2e_step():
+        for dp, (hh, ht) in zip(dps, host):
+            dp.ms.h_layer.copy_(hh, non_blocking=True)
+            for d, h in zip(dp.ms.tracers, ht):
+                d.copy_(h, non_blocking=True)
+        batch.step(1, st)
+        for dp, (_, ht) in zip(dps, host):
+            for d, h in zip(dp.ms.tracers, ht):
+                h.copy_(d, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
+    cells = sum(p.nx * p.ny * p.nz for p in ps)
+    ntr = ps[0].ntr
+    return {"value": batch.updates * world / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 8 * cells * (1 + ntr),
+            "d2h_bytes_per_step": 8 * cells * ntr, "ms_per_step": ms, "host_memory": "pinned"}
+
+
 def _uuid(local_rank):
     try:
         import torch
@@ -462,7 +711,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="config1", choices=["config0", "config1", "config3"])
+    ap.add_argument("--config", default="config1", choices=["config0", "config1", "config3", "config4"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: a generated domain of that size instead of --config")
     ap.add_argument("--no-e2e", action="store_true")
@@ -475,6 +724,8 @@ def main():
     rank, world, local_rank = _rank_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.config == "config4":
+        return run_domains(args, rank, world, local_rank)
     return run_b200(args, rank, world, local_rank)
 
 

@@ -232,6 +232,90 @@ REDI_B200_API int redi_b200_opt_launch_noalloc(
     const double* dx_cv, const double* idxCu, const double* idyCv, const double* areaT, double* tr_snap,
     void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Many independent regional domains stepped by one persistent kernel (no
+ * counterpart in the reference, whose driver steps one domain per call). The
+ * step of every domain (redi_calc_coeffs then redi_apply_flux for all of its
+ * tracers) is cut into tiles of columns, faces and cells; one grid of resident
+ * blocks drains that work queue, largest domains first, each tile starting
+ * once the previous stage of its own domain is complete. Per domain the
+ * results equal those of redi_b200_calc_coeffs + redi_b200_apply_flux on a
+ * handle of the same precision, bit for bit.
+ * ------------------------------------------------------------------------- */
+#define REDI_B200_STATUS_TIMEOUT 1 /* a tile waited longer than the wait limit */
+
+/* One domain: what redi_b200_calc_coeffs and redi_b200_apply_flux take. The
+ * per-face diffusivities are required (khtr_u_ext / khtr_v_ext non-NULL); ms
+ * needs 2..64 tracers with T and S registered. All arrays stay owned by the
+ * caller and must outlive the batch; their addresses are baked into it. */
+typedef struct redi_b200_domain {
+    redi_b200_grid grid;
+    redi_b200_metrics metrics;
+    redi_b200_eos eos;
+    redi_b200_state ms;
+    const double* khtr_u_ext;
+    const double* khtr_v_ext;
+    redi_b200_bc bc;
+    double dt;
+} redi_b200_domain;
+
+typedef struct redi_b200_batch redi_b200_batch;
+
+/* Builds the batch: Phase-A coefficient slots and scratch per domain, the work
+ * queue, and the persistent grid (as many 128-thread blocks as are resident on
+ * the current device). tile_bx x tile_by (= 128) is the cell tile of the
+ * gather, chunk (4, 8, 16) its vertical chunk. use_graph != 0 captures the step
+ * (counter reset + persistent kernel) in a CUDA graph on the first
+ * redi_b200_batch_step and replays it afterwards. Synchronises the device. */
+REDI_B200_API int redi_b200_batch_create(int ndomains, const redi_b200_domain* domains, int precision, int tile_bx,
+                                         int tile_by, int chunk, int use_graph, redi_b200_batch** out);
+
+/* One step of every domain, stream-ordered on stream; does not synchronise. */
+REDI_B200_API int redi_b200_batch_step(redi_b200_batch* b, void* stream);
+
+/* Outcome of the last step (synchronous read): status 0 or
+ * REDI_B200_STATUS_TIMEOUT, with the domain and stage (0 column state,
+ * 1 neutral sweep, 2 tracer reconstruction, 3 + 2g / 4 + 2g face flux / gather
+ * of tracer pair g) of the first tile that gave up; bad = fluxes the gather
+ * found out of order (0 for coefficients made in the step). Any out pointer
+ * but status may be NULL. After a timeout the step's results are incomplete. */
+REDI_B200_API int redi_b200_batch_status(const redi_b200_batch* b, int* status, int* domain, int* stage, int* bad);
+
+/* Launch shape of an existing batch (tile and chunk as in
+ * redi_b200_batch_create; occupancy = resident blocks per SM the kernel's
+ * registers are budgeted for, 4, 5 or 6, 0 keeps the current one, 4 at
+ * creation). Results do not depend on it. Rebuilds the work queue, keeps every
+ * domain's memory; synchronises the device. get_tuning also returns the
+ * persistent grid size (blocks). */
+REDI_B200_API int redi_b200_batch_set_tuning(redi_b200_batch* b, int tile_bx, int tile_by, int chunk, int occupancy);
+REDI_B200_API int redi_b200_batch_get_tuning(const redi_b200_batch* b, int* tile_bx, int* tile_by, int* chunk,
+                                             int* occupancy, int* grid);
+
+/* Per-stage accounting of the last step (off by default): with on != 0 the
+ * kernel sums, per stage kind (0 column state, 1 neutral sweep, 2 tracer
+ * reconstruction, 3 face flux, 4 gather), the time blocks waited for
+ * predecessors and spent on tiles (ms, summed over blocks) and the tiles done.
+ * stage_times synchronises the device; any out array may be NULL. */
+REDI_B200_API int redi_b200_batch_set_accounting(redi_b200_batch* b, int on);
+REDI_B200_API int redi_b200_batch_stage_times(const redi_b200_batch* b, double* wait_ms, double* busy_ms,
+                                              long long* tiles);
+
+/* Longest time a tile waits for its predecessors, in ns (default 2e9). */
+REDI_B200_API int redi_b200_batch_set_wait_limit(redi_b200_batch* b, long long ns);
+
+/* Fault injection for tests: hold != 0 keeps the domain's first stage waiting
+ * on a release flag that nothing sets while the step runs, so the step ends
+ * with REDI_B200_STATUS_TIMEOUT after the wait limit. */
+REDI_B200_API int redi_b200_batch_hold(redi_b200_batch* b, int domain, int hold);
+
+/* Tracer-cell updates per step (physical cells x layers x tracers, summed),
+ * and the number of tiles in the work queue. */
+REDI_B200_API long long redi_b200_batch_updates(const redi_b200_batch* b);
+REDI_B200_API long long redi_b200_batch_items(const redi_b200_batch* b);
+
+/* Frees the batch's device memory and graph. NULL is accepted. */
+REDI_B200_API int redi_b200_batch_destroy(redi_b200_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

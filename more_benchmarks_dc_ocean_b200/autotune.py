@@ -123,3 +123,41 @@ def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, int, int]]] = None, 
     set_tuning(*best)
     _store(dp, prec, best)
     return {"best": best, "ms": {f"{a}x{b}/ch{c}": round(v, 4) for (a, b, c), v in times.items()}, "cached": False}
+
+
+# Gather tiles of the persistent multi-domain kernel: its blocks are 128 threads.
+BATCH_TILES: Tuple[Tuple[int, int], ...] = ((32, 4), (16, 8))
+BATCH_OCCUPANCY: Tuple[int, ...] = (4, 5, 6)
+K_DOMAIN_PERSISTENT = 8
+
+
+def tune_batch(batch, candidates: Optional[Iterable[Tuple[int, int, int]]] = None, reps: int = 2,
+               stream=None) -> dict:
+    """Time whole batch steps for every (bx, by, chunk, occupancy) candidate and keep the fastest.
+
+    The persistent kernel runs every stage of every domain, so the candidate is
+    judged on the full step (its tracers are advanced in place). Returns
+    {"best": (bx, by, chunk, occupancy), "ms": {candidate: ms per step}}.
+    """
+    import torch
+
+    from . import ocean_redi as R
+
+    L = _bind(R.lib())
+    cands = list(candidates) if candidates is not None else [(bx, by, c, o) for (bx, by) in BATCH_TILES
+                                                             for c in CHUNKS for o in BATCH_OCCUPANCY]
+    times = {}
+    for cand in cands:
+        batch.set_tuning(cand[:2], cand[2], cand[3] if len(cand) > 3 else 0)
+        batch.step(1, stream)  # graph capture + warm-up
+        torch.cuda.synchronize()
+        L.redi_b200_profile_begin()
+        batch.step(reps, stream)
+        kt = (C.c_double * 16)()
+        kc = (C.c_ulonglong * 16)()
+        L.redi_b200_profile_end(kt, kc, 16)
+        times[cand] = kt[K_DOMAIN_PERSISTENT] / max(1, kc[K_DOMAIN_PERSISTENT])
+    best = min(times, key=times.get)
+    batch.set_tuning(best[:2], best[2], best[3] if len(best) > 3 else 0)
+    return {"best": best, "ms": {"x".join(map(str, k[:2])) + f"/ch{k[2]}" + (f"/occ{k[3]}" if len(k) > 3 else ""):
+                                 round(v, 4) for k, v in times.items()}}

@@ -1,6 +1,6 @@
 """Build the sm_100a shared library (libredi_b200.so) in-tree with nvcc.
 
-The FP64 kernels (redi_plain.cu) are compiled with FMA contraction off so their
+The kernels (redi_plain.cu, redi_domains.cu) are compiled with FMA contraction off so their
 arithmetic is the reference's IEEE sequence; everything is compiled for
 sm_100a only (`-gencode arch=compute_100a,code=sm_100a`).
 """
@@ -26,6 +26,7 @@ SOURCES = [
     ("redi_plain.cu", ["-fmad=false"]),
     ("redi_capi.cu", []),
     ("redi_noalloc.cu", []),
+    ("redi_domains.cu", ["-fmad=false"]),
 ]
 
 

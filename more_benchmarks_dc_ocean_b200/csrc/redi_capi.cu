@@ -149,7 +149,6 @@ int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch&
     const size_t flux = redi::flux_bytes<P>(in.nx, in.ny, in.nz, redi::tracer_group(batch));
     cudaError_t e = ws.reserve(recon + flux);
     if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (phase B)");
-    const size_t ncol = (size_t)in.nx * in.ny;
     const size_t ns1 = (size_t)(2 * in.nz + 1);
     using Flux = typename P::Flux;
     Flux* Fu = reinterpret_cast<Flux*>(static_cast<char*>(ws.data()) + recon);
@@ -159,7 +158,8 @@ int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch&
         redi::ReconArgsT<P> rc{};
         rc.nx = in.nx; rc.ny = in.ny; rc.nz = in.nz; rc.ntr = nt; rc.h = in.h;
         rc.ti = reinterpret_cast<double*>(ws.data());
-        rc.ppm = reinterpret_cast<typename P::Ppm*>(rc.ti + (size_t)nt * ncol * (in.nz + 1));
+        rc.ppm = reinterpret_cast<typename P::Ppm*>(static_cast<char*>(ws.data()) +
+                                                    redi::recon_ppm_offset(in.nx, in.ny, in.nz, nt));
         redi::FaceFluxArgsT<P> ff{};
         ff.nx = in.nx; ff.ny = in.ny; ff.nz = in.nz; ff.ntr = nt;
         ff.nghost = in.nghost; ff.nxp = in.nxp; ff.nyp = in.nyp;

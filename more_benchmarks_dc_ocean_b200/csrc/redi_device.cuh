@@ -19,6 +19,18 @@
 
 namespace redi {
 
+// Load paths. LdNC: the read-only (non-coherent) cache path, for data no
+// thread of the running kernel writes. LdCG: cached in L2 only, coherent
+// across the blocks of a running kernel, for data produced inside it.
+struct LdNC {
+    template <class T>
+    __device__ static __forceinline__ T ld(const T* p) { return __ldg(p); }
+};
+struct LdCG {
+    template <class T>
+    __device__ static __forceinline__ T ld(const T* p) { return __ldcg(p); }
+};
+
 constexpr double kGravity = 9.80665;    // redi/constants.F90:19
 constexpr double kHDivEps = 1.0e-20;    // redi/constants.F90:21
 constexpr double kHNeglect = 1.0e-30;   // ocean_redi.F90:242
@@ -123,9 +135,10 @@ struct alignas(32) IfcState {
     double T, S, dRdT, dRdS;
 };
 
+template <class LD>
 __device__ __forceinline__ IfcState load_ifc(const IfcState* p) {
     const double2* q = reinterpret_cast<const double2*>(p);
-    double2 a = __ldg(q), b = __ldg(q + 1);
+    double2 a = LD::ld(q), b = LD::ld(q + 1);
     IfcState r;
     r.T = a.x; r.S = a.y; r.dRdT = b.x; r.dRdS = b.y;
     return r;
@@ -170,9 +183,10 @@ __device__ __forceinline__ PpmLayer make_ppm_layer(double alk, double ark, doubl
     return q;
 }
 
+template <class LD>
 __device__ __forceinline__ PpmLayer load_ppm(const PpmLayer* p) {
     const double2* q = reinterpret_cast<const double2*>(p);
-    double2 a = __ldg(q), b = __ldg(q + 1);
+    double2 a = LD::ld(q), b = LD::ld(q + 1);
     PpmLayer r;
     r.aL = a.x; r.dA = a.y; r.a6o3 = b.x; r.B = b.y;
     return r;

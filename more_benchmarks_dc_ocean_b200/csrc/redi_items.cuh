@@ -1,0 +1,721 @@
+// Per-item device functions of the Redi step: one column, one face or one cell
+// per call. Shared by the standalone kernels (redi_plain.cu) and the
+// multi-domain persistent kernel (redi_domains.cu). LD is the load path
+// (LdNC for data no running thread writes, LdCG for data produced inside the
+// running kernel). Include only from translation units compiled with FMA
+// contraction off.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "redi_device.cuh"
+#include "redi_kernels.h"
+
+namespace redi {
+namespace plain {
+
+// ---------------------------------------------------------------------------
+// Streaming top-down PPM interface reconstruction (redi_interface_scalar,
+// ocean_redi.F90:231-254) of NS scalars that share one thickness column.
+//
+// Layers are pulled from the surface down through `load(t, h, s)`, t = 1..nk
+// top-down; edge(t) needs layers t-2..t+1, so a four-layer register window
+// replaces the reference's column arrays. `emit(t, e, s_above)` receives
+// interface t (1..nk+1), its NS edge values, and the NS means of the layer
+// just above it (layer t-1; undefined for t = 1).
+// ---------------------------------------------------------------------------
+template <int NS, class Load, class Emit>
+__device__ __forceinline__ void stream_edges(int nk, Load load, Emit emit) {
+    double hA = 0.0, hB, hC, hD = 0.0;  // h(t-2), h(t-1), h(t), h(t+1)
+    double sB[NS], sC[NS], sD[NS];      // layer scalars t-1, t, t+1
+    double dB[NS], dC[NS];              // PLM slopes of layers t-1, t
+    double e[NS];
+
+    // t = 1: edge(1) = tr(1) - 0.5*diff(1), diff(1) = 0.
+    load(1, hC, sC);
+    if (nk >= 2) load(2, hD, sD);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+        dC[n] = 0.0;
+        e[n] = sC[n] - 0.5 * dC[n];
+        sB[n] = 0.0;
+    }
+    emit(1, e, sB);
+
+    for (int t = 2; t <= nk; ++t) {
+        // shift the window down one layer: (t-1) <- t, t <- t+1
+        hA = (t >= 3) ? hB : hA;
+        hB = hC;
+        hC = hD;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+            sB[n] = sC[n];
+            sC[n] = sD[n];
+            dB[n] = dC[n];
+        }
+        if (t + 1 <= nk) load(t + 1, hD, sD);
+        // diff(t): PLM slope for 2 <= t <= nk-1, PCM (0) at t = nk.
+        if (t <= nk - 1) {
+            const PlmGeom pg = plm_geom(hB, hC, hD);
+#pragma unroll
+            for (int n = 0; n < NS; ++n) dC[n] = plm_slope(pg, sB[n], sC[n], sD[n]);
+        } else {
+#pragma unroll
+            for (int n = 0; n < NS; ++n) dC[n] = 0.0;
+        }
+        const double hkm1 = (t >= 3) ? hA : hB;   // h(max(1, t-2))
+        const double hkp2 = (t + 1 <= nk) ? hD : hC;  // h(min(nk, t+1))
+        const EdgeGeom eg = edge_geom(hkm1, hB, hC, hkp2, kHNeglect);
+#pragma unroll
+        for (int n = 0; n < NS; ++n) e[n] = ppm_edge(eg, sB[n], sC[n], dB[n], dC[n]);
+        emit(t, e, sB);
+    }
+    // edge(nk+1) = tr(nk) + 0.5*diff(nk), diff(nk) = 0.
+#pragma unroll
+    for (int n = 0; n < NS; ++n) e[n] = sC[n] + 0.5 * dC[n];
+    emit(nk + 1, e, sC);
+}
+
+// ---------------------------------------------------------------------------
+// Phase A, step 1: per-column interface state (redi_build_column,
+// ocean_redi.F90:609-654), written in [interface][column] order.
+// ---------------------------------------------------------------------------
+template <class LD>
+__device__ __forceinline__ void column_state_item(const ColumnStateArgs& a, int col) {
+    const int ncol = a.nx * a.ny;
+    const int nz = a.nz;
+    const double* __restrict__ h = a.h + col;
+    const double* __restrict__ th = a.th + col;
+    const double* __restrict__ sh = a.sh + col;
+    IfcState* __restrict__ ifc = a.ifc + col;
+    double* __restrict__ pint = a.pint + col;
+
+    const EosLin eos = a.eos;
+    const double dsv_dt = eos.alpha_T / (eos.rho0 * eos.rho0);  // ocean_eos.F90:511
+    const double dsv_ds = -eos.beta_S / (eos.rho0 * eos.rho0);  // ocean_eos.F90:512
+    const double grho = kGravity * eos.rho0;
+    double P = 0.0;
+    double h_layer_above = 0.0;
+
+    auto load = [&](int t, double& hv, double (&sv)[2]) {
+        const size_t off = (size_t)(nz - t) * ncol;  // native k = nz+1-t (1-based)
+        const double hk = LD::ld(h + off);
+        const double he = fmax(hk, kHDivEps);
+        hv = hk;
+        sv[0] = LD::ld(th + off) / he;
+        sv[1] = LD::ld(sh + off) / he;
+    };
+    auto emit = [&](int t, const double (&e)[2], const double (&)[2]) {
+        if (t >= 2) P = P + grho * h_layer_above;  // Pint(t) = Pint(t-1) + g*rho0*h(t-1)
+        const double rho_i = eos.rho0 + eos.beta_S * (e[1] - eos.S_ref) - eos.alpha_T * (e[0] - eos.T_ref);
+        double2* q = reinterpret_cast<double2*>(ifc + (size_t)(t - 1) * ncol);
+        q[0] = make_double2(e[0], e[1]);
+        q[1] = make_double2(-(rho_i * rho_i) * dsv_dt, -(rho_i * rho_i) * dsv_ds);
+        pint[(size_t)(t - 1) * ncol] = P;
+        if (t <= nz) h_layer_above = LD::ld(h + (size_t)(nz - t) * ncol);
+    };
+    stream_edges<2>(nz, load, emit);
+}
+
+// ---------------------------------------------------------------------------
+// Phase A, step 2: the continuous neutral-surface sweep per face
+// (redi_neutral_positions_continuous + redi_face_coeffs, ocean_redi.F90:307-464,
+// 656-692) and the slot writes of redi_calc_coeffs_x/_y (:694-812).
+//
+// Each column is read through a three-interface register window anchored at
+// km1 = max(k-1, 1) (the reference's klm1/krm1): interfaces km1, km1+1 and
+// km1+2 with their pressures. The pointer's own interface is km1 (k = 1) or
+// km1+1 (k >= 2). When a pointer advances the window slides by one and one
+// interface is fetched ahead, so a step waits on no load it has just issued.
+// The two search directions share one code path: the searched column S and
+// the anchor column A are selected per step (with the reference's asymmetric
+// `dRhoTop > 0` / `dRhoTop >= 0` tests kept).
+// ---------------------------------------------------------------------------
+struct ColWin {
+    IfcState a, b, c;   // interfaces km1, km1+1, km1+2 (1-based)
+    double pa, pb, pc;  // pressures at the same interfaces
+    int k;              // the pointer (1-based, 1..nk+1)
+};
+
+template <class LD>
+__device__ __forceinline__ void win_init(ColWin& w, const IfcState* X, const double* P, int nk, size_t ld) {
+    w.k = 1;
+    const int i1 = min(1, nk), i2 = min(2, nk);
+    w.a = load_ifc<LD>(X);
+    w.b = load_ifc<LD>(X + (size_t)i1 * ld);
+    w.c = load_ifc<LD>(X + (size_t)i2 * ld);
+    w.pa = LD::ld(P);
+    w.pb = LD::ld(P + (size_t)i1 * ld);
+    w.pc = LD::ld(P + (size_t)i2 * ld);
+}
+
+// k -> k+1: the anchor km1 moves only when k was >= 2.
+template <class LD>
+__device__ __forceinline__ void win_advance(ColWin& w, const IfcState* X, const double* P, int nk, size_t ld) {
+    if (w.k >= 2) {
+        w.a = w.b;
+        w.b = w.c;
+        w.pa = w.pb;
+        w.pb = w.pc;
+        const int inext = min(w.k + 1, nk);  // 0-based index of interface km1_new + 2
+        w.c = load_ifc<LD>(X + (size_t)inext * ld);
+        w.pc = LD::ld(P + (size_t)inext * ld);
+    }
+    w.k += 1;
+}
+
+__device__ __forceinline__ IfcState sel(bool c, const IfcState& x, const IfcState& y) {
+    IfcState r;
+    r.T = c ? x.T : y.T;
+    r.S = c ? x.S : y.S;
+    r.dRdT = c ? x.dRdT : y.dRdT;
+    r.dRdS = c ? x.dRdS : y.dRdS;
+    return r;
+}
+
+__device__ __forceinline__ IfcState win_own(const ColWin& w) { return sel(w.k == 1, w.a, w.b); }
+
+template <class P, class LD>
+__device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int t) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    const size_t ld = (size_t)nx * ny;  // interface stride of the scratch
+    int colL, colR, fo, nface;
+    size_t fstride;
+    if (dir == 0) {  // Fortran faces i = 2..nx, j = 1..ny
+        nface = (nx - 1) * ny;
+        if (t >= nface) return;
+        const int j = t / (nx - 1), fi = 1 + t % (nx - 1);
+        colL = (fi - 1) + nx * j;
+        colR = fi + nx * j;
+        fo = fi + (nx + 1) * j;
+        fstride = (size_t)(nx + 1) * ny;
+    } else {  // Fortran faces j = 2..ny, i = 1..nx
+        nface = nx * (ny - 1);
+        if (t >= nface) return;
+        const int fj = 1 + t / nx, i = t % nx;
+        colL = i + nx * (fj - 1);
+        colR = i + nx * fj;
+        fo = i + nx * fj;
+        fstride = (size_t)nx * (ny + 1);
+    }
+    using Po = typename P::Po;
+    using Ko = typename P::Ko;
+    using He = typename P::He;
+    const FaceOutT<P> o = dir == 0 ? a.u : a.v;
+    Po* __restrict__ PoL = o.PoL + fo;
+    Po* __restrict__ PoR = o.PoR + fo;
+    Ko* __restrict__ KoL = o.KoL + fo;
+    Ko* __restrict__ KoR = o.KoR + fo;
+    He* __restrict__ hEff = o.hEff + fo;
+    const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
+
+    if (!(wet > 0.0)) {  // ocean_redi.F90:722-730: inert coefficients
+        for (int s = 0; s < ns; ++s) {
+            PoL[s * fstride] = Po(0);
+            PoR[s * fstride] = Po(0);
+            KoL[s * fstride] = Ko(1);
+            KoR[s * fstride] = Ko(1);
+        }
+        for (int s = 0; s < ns - 1; ++s) hEff[s * fstride] = He(0);
+        return;
+    }
+
+    const IfcState* XL = a.ifc + colL;
+    const IfcState* XR = a.ifc + colR;
+    const double* PL = a.pint + colL;
+    const double* PR = a.pint + colR;
+    const double pa_to_h = 1.0 / (kGravity * a.rho0);
+    const int nk = nz;
+
+    ColWin wl, wr;
+    win_init<LD>(wl, XL, PL, nk, ld);
+    win_init<LD>(wr, XR, PR, nk, ld);
+    double lastP_left = 0.0, lastP_right = 0.0;
+    int lastK_left = 1, lastK_right = 1;
+    bool reached_bottom = false, search_left = false, search_right = false;
+    double absL_prev = 0.0, absR_prev = 0.0;
+
+    for (int ks = 1; ks <= ns; ++ks) {
+        const int kl = wl.k, kr = wr.k;
+        const double dRho = secant_drho(win_own(wr), win_own(wl));
+        if (!reached_bottom) {
+            if (dRho < 0.0) {
+                search_left = true;
+                search_right = false;
+            } else if (dRho > 0.0) {
+                search_right = true;
+                search_left = false;
+            } else if (kl + kr == 2) {
+                search_left = true;
+                search_right = false;
+            } else {
+                search_left = !search_left;
+                search_right = !search_right;
+            }
+        }
+        // Exactly one direction is set. S: searched column, A: anchor column
+        // (selected field by field so both windows stay in registers).
+        const bool L = search_left;
+        const IfcState Sa = sel(L, wl.a, wr.a), Sb = sel(L, wl.b, wr.b);
+        const double Spa = L ? wl.pa : wr.pa, Spb = L ? wl.pb : wr.pb, Spc = L ? wl.pc : wr.pc;
+        const int Sk = L ? kl : kr;
+        const IfcState anc = L ? (kr == 1 ? wr.a : wr.b) : (kl == 1 ? wl.a : wl.b);
+        const double Apa = L ? wr.pa : wl.pa, Apb = L ? wr.pb : wl.pb, Apc = L ? wr.pc : wl.pc;
+        const int ka = L ? kr : kl;
+        const double dRhoTop = secant_drho(Sa, anc);
+        const double dRhoBot = secant_drho(Sb, anc);
+        const int km1 = Sk - 1 > 1 ? Sk - 1 : 1;
+        double po_s;
+        const bool top_zero = (L ? (dRhoTop > 0.0) : (dRhoTop >= 0.0)) || kr + kl == 2;
+        if (top_zero) po_s = 0.0;
+        else if (dRhoTop >= dRhoBot) po_s = 1.0;
+        else po_s = interpolate_position(dRhoTop, Spa, dRhoBot, Spb);
+        int ko_s = km1;
+        bool carried = false;
+        if (po_s >= 1.0 && km1 < nk) {
+            ko_s = km1 + 1;
+            po_s = po_s - 1.0;
+            carried = true;
+        }
+        const int lastK_s = L ? lastK_left : lastK_right;
+        const double lastP_s = L ? lastP_left : lastP_right;
+        bool backstop = false;
+        if ((double)(ko_s - lastK_s) + (po_s - lastP_s) < 0.0) {
+            po_s = lastP_s;
+            ko_s = lastK_s;
+            backstop = true;
+        }
+        // absolute position of the searched side (redi_absolute_position)
+        double abs_s;
+        if (backstop) abs_s = L ? absL_prev : absR_prev;
+        else if (carried) abs_s = Spb + po_s * (Spc - Spb);
+        else abs_s = Spa + po_s * (Spb - Spa);
+        // anchor side: its own interface, or the bed once exhausted
+        double po_a, abs_a;
+        int ko_a;
+        if (ka <= nk) {
+            po_a = 0.0;
+            ko_a = ka;
+            abs_a = (ka == 1) ? Apa + po_a * (Apb - Apa) : Apb + po_a * (Apc - Apb);
+        } else {
+            po_a = 1.0;
+            ko_a = nk;
+            abs_a = Apa + po_a * (Apb - Apa);  // km1 = nk: interfaces nk, nk+1
+        }
+        if (ka <= nk) {
+            if (L) win_advance<LD>(wr, XR, PR, nk, ld);
+            else   win_advance<LD>(wl, XL, PL, nk, ld);
+        } else {
+            reached_bottom = true;
+            search_left = !L;
+            search_right = L;
+        }
+        const double pol = L ? po_s : po_a, por = L ? po_a : po_s;
+        const int kol = L ? ko_s : ko_a, kor = L ? ko_a : ko_s;
+        const double absL = L ? abs_s : abs_a, absR = L ? abs_a : abs_s;
+        lastK_left = kol;
+        lastP_left = pol;
+        lastK_right = kor;
+        lastP_right = por;
+        const size_t so = (size_t)(ks - 1) * fstride;
+        PoL[so] = Po(pol);
+        PoR[so] = Po(por);
+        KoL[so] = Ko(kol);
+        KoR[so] = Ko(kor);
+        if (ks > 1) {  // harmonic-mean effective thickness (:452-462), Pa -> m (:688-691)
+            const double hL = absL - absL_prev;
+            const double hR = absR - absR_prev;
+            double he = 0.0;
+            if (hL + hR > 0.0) he = 2.0 * hL * hR / (hL + hR);
+            hEff[so - fstride] = He(he * pa_to_h);
+        }
+        absL_prev = absL;
+        absR_prev = absR;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phase B, step 1: per-column tracer reconstruction for a group of NT tracers
+// (redi_tracer_column, ocean_redi.F90:852-891). Writes, per tracer, the nz+1
+// interface values Tint and the nz prepared PPM layers in [layer][column]
+// order, so that threads of neighbouring columns touch neighbouring addresses.
+// ---------------------------------------------------------------------------
+template <class P>
+__device__ __forceinline__ void store_ppm(typename P::Ppm* p, const PpmLayer& q);
+template <>
+__device__ __forceinline__ void store_ppm<PlainPrec>(PpmLayer* p, const PpmLayer& q) {
+    double2* d = reinterpret_cast<double2*>(p);
+    d[0] = make_double2(q.aL, q.dA);
+    d[1] = make_double2(q.a6o3, q.B);
+}
+template <>
+__device__ __forceinline__ void store_ppm<MixedPrec>(PpmLayerF* p, const PpmLayer& q) {
+    *reinterpret_cast<float4*>(p) = make_float4((float)q.aL, (float)q.dA, (float)q.a6o3, (float)q.B);
+}
+
+template <int NT, class P, class LD>
+__device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid) {
+    const int ncol = a.nx * a.ny;
+    const int ngroups = (a.ntr + NT - 1) / NT;
+    if (gid >= ncol * ngroups) return;
+    const int col = gid % ncol;
+    const int g = gid / ncol;
+    const int tr0 = g * NT;
+    const int nt = min(NT, a.ntr - tr0);
+    const int nz = a.nz;
+    const double* __restrict__ h = a.h + col;
+    const double* htr[NT];
+    double* ti[NT];
+    typename P::Ppm* ppm[NT];
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        const int tr = tr0 + (n < nt ? n : 0);
+        htr[n] = a.htr[tr] + col;
+        ti[n] = a.ti + (size_t)tr * ncol * (nz + 1) + col;
+        ppm[n] = a.ppm + (size_t)tr * ncol * nz + col;
+    }
+    double e_prev[NT];
+
+    auto load = [&](int t, double& hv, double (&sv)[NT]) {
+        const size_t off = (size_t)(nz - t) * ncol;
+        const double hk = LD::ld(h + off);
+        const double he = fmax(hk, kHDivEps);
+        hv = hk;
+#pragma unroll
+        for (int n = 0; n < NT; ++n) sv[n] = LD::ld(htr[n] + off) / he;
+    };
+    auto emit = [&](int t, const double (&e)[NT], const double (&s_above)[NT]) {
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            if (n < nt) {
+                ti[n][(size_t)(t - 1) * ncol] = e[n];
+                if (t >= 2) {  // layer t-1 is complete: limit its edges
+                    double alk = e_prev[n], ark = e[n];
+                    const double tlk = s_above[n];
+                    ppm_limit(alk, ark, tlk);
+                    store_ppm<P>(ppm[n] + (size_t)(t - 2) * ncol, make_ppm_layer(alk, ark, tlk));
+                }
+            }
+            e_prev[n] = e[n];
+        }
+    };
+    stream_edges<NT>(nz, load, emit);
+}
+
+// ---------------------------------------------------------------------------
+// Phase B, step 2: the along-neutral flux of every face, computed once
+// (redi_face_flux + redi_sublayer_dT, ocean_redi.F90:893-925, 1037-1092).
+//
+// One thread per interior, non-wall face; all lanes of a warp walk the same
+// sublayer ks, so each coefficient load is one contiguous row. The flux
+// flx(ks) = dT * hEff * coef of every tracer is stored in F[tracer][ks][face];
+// sublayers with hEff == 0 store +0.0. The reference evaluates each interior
+// face twice (once from each adjacent cell, with identical operands and hence
+// identical bits); here it is evaluated once and read by both cells.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double interp(double P, double a, double b) { return (1.0 - P) * a + P * b; }
+
+// Layer mean of the PPM parabola and the flux product, per precision.
+template <class P>
+struct FluxOps;
+
+template <>
+struct FluxOps<PlainPrec> {
+    using Mean = double;
+    template <class LD>
+    __device__ static __forceinline__ double mean(double xL, double xR, const PpmLayer* p) {
+        return ppm_ave(xL, xR, load_ppm<LD>(p));
+    }
+    __device__ static __forceinline__ double flux(double dT, double he, double coef) { return dT * he * coef; }
+};
+
+template <>
+struct FluxOps<MixedPrec> {
+    using Mean = float;
+    // redi_ppm_ave in FP32; the branch (a discrete decision) is taken on the
+    // FP64 positions exactly as in the plain form.
+    template <class LD>
+    __device__ static __forceinline__ float mean(double xL, double xR, const PpmLayerF* p) {
+        const float4 q = LD::ld(reinterpret_cast<const float4*>(p));  // aL, dA, a6o3, B
+        const float xl = (float)xL, xr = (float)xR;
+        const double dx = xR - xL;
+        if (dx > 0.0 && dx <= 1.0) {
+            const float xave = 0.5f * (xr + xl);
+            return (q.x + xave * q.w) - q.z * (xr * xr + xr * xl + xl * xl);
+        }
+        const float a6 = 3.0f * q.z;
+        return q.x + q.y * xr + a6 * xr * (1.0f - xr);
+    }
+    __device__ static __forceinline__ float flux(double dT, float he, double coef) {
+        return (float)dT * he * (float)coef;
+    }
+};
+
+template <int NT, class P, class LD>
+__device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, int t, int tr0) {
+    using Ops = FluxOps<P>;
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    const size_t ncol = (size_t)nx * ny;
+    int colL, colR, fo;
+    size_t fstride;
+    if (dir == 0) {  // Fortran faces I = 2..nx, excluding walls
+        if (t >= (nx - 1) * ny) return;
+        const int j = t / (nx - 1), fi = 1 + t % (nx - 1);
+        const int I = fi + 1;
+        if ((a.wall_w && I == a.nghost + 1) || (a.wall_e && I == a.nghost + a.nxp + 1)) return;
+        colL = (fi - 1) + nx * j;
+        colR = fi + nx * j;
+        fo = fi + (nx + 1) * j;
+        fstride = (size_t)(nx + 1) * ny;
+    } else {  // Fortran faces J = 2..ny, excluding walls
+        if (t >= nx * (ny - 1)) return;
+        const int fj = 1 + t / nx, i = t % nx;
+        const int J = fj + 1;
+        if ((a.wall_s && J == a.nghost + 1) || (a.wall_n && J == a.nghost + a.nyp + 1)) return;
+        colL = i + nx * (fj - 1);
+        colR = i + nx * fj;
+        fo = i + nx * fj;
+        fstride = (size_t)nx * (ny + 1);
+    }
+    const FaceInT<P>& c = dir == 0 ? a.u : a.v;
+    const typename P::He* __restrict__ hEff = c.hEff + fo;
+    const typename P::Po* __restrict__ PoL = c.PoL + fo;
+    const typename P::Po* __restrict__ PoR = c.PoR + fo;
+    const typename P::Ko* __restrict__ KoL = c.KoL + fo;
+    const typename P::Ko* __restrict__ KoR = c.KoR + fo;
+    const double* kh = dir == 0 ? a.khtr_u : a.khtr_v;
+    const double khv = kh ? LD::ld(kh + fo) : a.khtr;
+    // ((dt*khtr)*dy)*idx, ocean_redi.F90:1156/1168
+    const double coef = a.dt * khv * LD::ld((dir == 0 ? a.dy_cu : a.dx_cv) + fo) *
+                        LD::ld((dir == 0 ? a.idxCu : a.idyCv) + fo);
+    const int nt = min(NT, a.ntr - tr0);
+    const double* tiL[NT];
+    const double* tiR[NT];
+    const typename P::Ppm* ppL[NT];
+    const typename P::Ppm* ppR[NT];
+    typename P::Flux* Fo[NT];
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+        const int tr = tr0 + (n < nt ? n : 0);
+        tiL[n] = a.ti + (size_t)tr * ncol * (nz + 1) + colL;
+        tiR[n] = a.ti + (size_t)tr * ncol * (nz + 1) + colR;
+        ppL[n] = a.ppm + (size_t)tr * ncol * nz + colL;
+        ppR[n] = a.ppm + (size_t)tr * ncol * nz + colR;
+        Fo[n] = (dir == 0 ? a.Fu : a.Fv) + (size_t)(tr - tr0) * (size_t)(ns - 1) * fstride + fo;
+    }
+
+    // Register rotation: while sublayer s is evaluated, hEff(s+1) and the
+    // bottom surface of s+1 (surface s+2) are already being fetched. The top
+    // surface of s is always the bottom surface of s-1.
+    using He = typename P::He;
+    bool have_t = false;  // tl/tr hold the tracer values at the top surface
+    int kl_t = min(max((int)LD::ld(KoL), 1), nz), kr_t = min(max((int)LD::ld(KoR), 1), nz);
+    double pl_t = LD::ld(PoL), pr_t = LD::ld(PoR);
+    He he_c = LD::ld(hEff);
+    int klr_c = LD::ld(KoL + fstride), krr_c = LD::ld(KoR + fstride);
+    double pl_c = LD::ld(PoL + fstride), pr_c = LD::ld(PoR + fstride);
+    double tl[NT], tr[NT];
+    for (int s = 0; s < ns - 1; ++s) {
+        const size_t s0 = (size_t)s * fstride;
+        He he_n = He(0);
+        int klr_n = 1, krr_n = 1;
+        double pl_n = 0.0, pr_n = 0.0;
+        if (s + 1 < ns - 1) {
+            const size_t s2 = s0 + 2 * fstride;
+            he_n = LD::ld(hEff + s0 + fstride);
+            klr_n = LD::ld(KoL + s2);
+            krr_n = LD::ld(KoR + s2);
+            pl_n = LD::ld(PoL + s2);
+            pr_n = LD::ld(PoR + s2);
+        }
+        const int kl_b = min(max(klr_c, 1), nz);
+        const int kr_b = min(max(krr_c, 1), nz);
+        const double pl_b = pl_c, pr_b = pr_c;
+        if (he_c == He(0)) {
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+                if (n < nt) Fo[n][s0] = typename P::Flux(0);
+            have_t = false;
+        } else {
+            if (!have_t) {
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    tl[n] = interp(pl_t, LD::ld(tiL[n] + (size_t)(kl_t - 1) * ncol), LD::ld(tiL[n] + (size_t)kl_t * ncol));
+                    tr[n] = interp(pr_t, LD::ld(tiR[n] + (size_t)(kr_t - 1) * ncol), LD::ld(tiR[n] + (size_t)kr_t * ncol));
+                }
+            }
+            const double xRl = pl_b + (double)(kl_b - kl_t);
+            const double xRr = pr_b + (double)(kr_b - kr_t);
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                const double bl = interp(pl_b, LD::ld(tiL[n] + (size_t)(kl_b - 1) * ncol), LD::ld(tiL[n] + (size_t)kl_b * ncol));
+                const double br = interp(pr_b, LD::ld(tiR[n] + (size_t)(kr_b - 1) * ncol), LD::ld(tiR[n] + (size_t)kr_b * ncol));
+                if (n < nt) {
+                    const typename Ops::Mean tlay = Ops::template mean<LD>(pl_t, xRl, ppL[n] + (size_t)(kl_t - 1) * ncol);
+                    const typename Ops::Mean trlay = Ops::template mean<LD>(pr_t, xRr, ppR[n] + (size_t)(kr_t - 1) * ncol);
+                    const double dT = guarded_dT(tr[n] - tl[n], br - bl, (double)(trlay - tlay));
+                    Fo[n][s0] = Ops::flux(dT, he_c, coef);
+                }
+                tl[n] = bl;
+                tr[n] = br;
+            }
+            have_t = true;
+        }
+        kl_t = kl_b;
+        kr_t = kr_b;
+        pl_t = pl_b;
+        pr_t = pr_b;
+        he_c = he_n;
+        klr_c = klr_n;
+        krr_c = krr_n;
+        pl_c = pl_n;
+        pr_c = pr_n;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phase B, step 3: per-cell flux divergence (redi_apply_flux_impl,
+// ocean_redi.F90:1094-1181).
+//
+// One thread per T-cell column; a block is a BX x BY tile of columns. The
+// reference adds, for each native layer of a cell, the flux of the W face
+// (sublayers ks ascending, -flx into layer nz+1-KoR), then E (+flx at
+// nz+1-KoL), S (-flx at KoR) and N (+flx at KoL) to dTr(k) starting from
+// zero, then hTr(k) += dTr(k)*(1/areaT). Along one face the cell-side Ko is
+// non-decreasing in ks (the sweep's monotonic-position backstop,
+// ocean_redi.F90:385-388, 424-427), so one face's contributions to a block of
+// CH layers form a contiguous run of sublayers. The kernel walks the column in
+// chunks of CH layers and, per chunk, folds the W, E, S and N runs that land in
+// it, in that order: every layer receives exactly the reference's additions in
+// the reference's sequence (stored zero fluxes of skipped sublayers add +0.0,
+// which leaves any dTr value unchanged: dTr starts at +0.0 and an IEEE sum or
+// difference never turns it into -0.0). Consecutive additions to one layer run
+// in a register. A flux whose cell-side layer lies behind the chunk (not
+// possible for sweep-produced coefficients) is counted in the device error
+// word and skipped.
+// ---------------------------------------------------------------------------
+template <int NT, int CH, class P, class LD>
+__device__ __forceinline__ void gather_run(const typename P::Flux* const (&F)[NT],
+                                           const typename P::Ko* __restrict__ KoS, size_t stride, bool left, int ns,
+                                           int& ptr, int k0, int k1, double (&dTr)[NT][CH], int& bad) {
+    // Sublayers are fetched U at a time (independent loads in flight), then
+    // consumed in order until the first one beyond the chunk.
+    constexpr int U = 4;
+    int cur = -1;
+    double acc[NT];
+    int s = ptr;
+    bool done = false;
+    while (!done && s < ns - 1) {
+        int kk[U];
+        double ff[U][NT];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int su = s + u;
+            if (su < ns - 1) {
+                const size_t so = (size_t)su * stride;
+                kk[u] = (int)LD::ld(KoS + so);
+#pragma unroll
+                for (int n = 0; n < NT; ++n) ff[u][n] = (double)LD::ld(F[n] + so);
+            } else {
+                kk[u] = 0x7fffffff;
+#pragma unroll
+                for (int n = 0; n < NT; ++n) ff[u][n] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (done) break;
+            const int k = kk[u];
+            if (k >= k1) {  // also the end of the face (s >= ns-1)
+                done = true;
+                break;
+            }
+            ++s;
+            if (k < k0) {
+                ++bad;
+                continue;
+            }
+            const int slot = k - k0;
+            if (slot != cur) {
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    if (cur >= 0) dTr[n][cur] = acc[n];
+                    acc[n] = dTr[n][slot];
+                }
+                cur = slot;
+            }
+#pragma unroll
+            for (int n = 0; n < NT; ++n) acc[n] = left ? acc[n] + ff[u][n] : acc[n] - ff[u][n];
+        }
+    }
+    ptr = s;
+    if (cur >= 0) {
+#pragma unroll
+        for (int n = 0; n < NT; ++n) dTr[n][cur] = acc[n];
+    }
+}
+
+template <int NT, int CH, class P, class LD>
+__device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, int j, int tr0) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    if (i >= nx || j >= ny) return;
+    const size_t ncol = (size_t)nx * ny;
+    const int col = i + nx * j;
+    const int nt = min(NT, a.ntr - tr0);
+    const int I = i + 1, J = j + 1;  // Fortran indices
+    const int wuf_w = a.nghost + 1, wuf_e = a.nghost + a.nxp + 1;
+    const int wvf_s = a.nghost + 1, wvf_n = a.nghost + a.nyp + 1;
+    const size_t ustride = (size_t)(nx + 1) * ny, vstride = (size_t)nx * (ny + 1);
+    // Faces in the reference order: W (u-face I, this cell RIGHT), E (u-face
+    // I+1, LEFT), S (v-face J, RIGHT), N (v-face J+1, LEFT).
+    const bool on[4] = {I >= 2 && !((a.wall_w && I == wuf_w) || (a.wall_e && I == wuf_e)),
+                        I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e)),
+                        J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n)),
+                        J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))};
+    const int fo[4] = {i + (nx + 1) * j, i + 1 + (nx + 1) * j, i + nx * j, i + nx * (j + 1)};
+    const double iaij = 1.0 / LD::ld(a.areaT + col);
+    int ptr[4] = {0, 0, 0, 0};
+    int bad = 0;
+    double dTr[NT][CH];
+    for (int k0 = 1; k0 <= nz; k0 += CH) {
+        const int k1 = min(k0 + CH, nz + 1);
+#pragma unroll
+        for (int n = 0; n < NT; ++n)
+#pragma unroll
+            for (int c = 0; c < CH; ++c) dTr[n][c] = 0.0;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            if (!on[f]) continue;
+            const bool u = f < 2, left = (f & 1) != 0;
+            const size_t stride = u ? ustride : vstride;
+            const typename P::Flux* F[NT];
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+                F[n] = (u ? a.Fu : a.Fv) + (size_t)(n < nt ? n : 0) * (size_t)(ns - 1) * stride + fo[f];
+            const FaceInT<P>& c = u ? a.u : a.v;
+            gather_run<NT, CH, P, LD>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1, dTr, bad);
+        }
+        // Layers k0..k1-1 are complete: hTr(knat) += dTr(knat) * (1/areaT), knat = nz + 1 - k.
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            if (n >= nt) break;
+            double* __restrict__ out = a.htr[tr0 + n] + col;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const int k = k0 + c;
+                if (k < k1) {
+                    const size_t o = (size_t)(nz - k) * ncol;
+                    out[o] = out[o] + dTr[n][c] * iaij;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+        if (on[f] && ptr[f] < ns - 1) ++bad;  // fluxes whose cell-side layer is beyond nz
+    if (bad && a.err) atomicAdd(a.err, bad);
+}
+
+}  // namespace plain
+}  // namespace redi

@@ -139,10 +139,14 @@ inline size_t phase_a_scratch(int nx, int ny, int nz) {
     const size_t nifc = (size_t)nx * ny * (nz + 1);
     return nifc * sizeof(IfcState) + nifc * sizeof(double);
 }
+// Byte offset of the PPM layers behind the interface values in a Phase-B
+// reconstruction buffer; 256-byte aligned, the layers are read as 16-byte vectors.
+inline size_t recon_ppm_offset(int nx, int ny, int nz, int ntr) {
+    return ((size_t)ntr * nx * ny * (nz + 1) * sizeof(double) + 255) & ~size_t(255);
+}
 template <class P>
 inline size_t recon_bytes(int nx, int ny, int nz, int ntr) {
-    const size_t ncol = (size_t)nx * ny;
-    return (size_t)ntr * ncol * ((nz + 1) * sizeof(double) + nz * sizeof(typename P::Ppm));
+    return recon_ppm_offset(nx, ny, nz, ntr) + (size_t)ntr * nx * ny * nz * sizeof(typename P::Ppm);
 }
 template <class P>
 inline size_t flux_bytes(int nx, int ny, int nz, int group) {

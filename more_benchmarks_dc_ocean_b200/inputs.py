@@ -178,10 +178,15 @@ def _bathymetry(nxp, nyp, nghost, dx, n_seamounts, land_target, seed, depth=4000
 def _box5(a: np.ndarray) -> np.ndarray:
     """5x5 moving average over the last two axes with edge replication."""
     p = np.pad(a, [(0, 0), (2, 2), (2, 2)], mode="edge")
-    c = np.cumsum(np.cumsum(p, axis=1), axis=2)
-    c = np.pad(c, [(0, 0), (1, 0), (1, 0)])
-    s = c[:, 5:, 5:] - c[:, :-5, 5:] - c[:, 5:, :-5] + c[:, :-5, :-5]
-    return s / 25.0
+    ny, nx = a.shape[1], a.shape[2]
+    r = p[:, 0:ny] + p[:, 1:ny + 1]  # separable running sums over contiguous slabs
+    for o in (2, 3, 4):
+        r += p[:, o:ny + o]
+    s = r[:, :, 0:nx] + r[:, :, 1:nx + 1]
+    for o in (2, 3, 4):
+        s += r[:, :, o:nx + o]
+    s /= 25.0
+    return s
 
 
 def make_problem(nx_phys: int, ny_phys: int, nz: int, *, n_seamounts: int = 6, land_fraction: float = 0.15,
@@ -274,11 +279,37 @@ def config4_shapes(seed: int = 20261203, n_domains: int = 64):
     return [(int(a), int(b), int(c)) for a, b, c in zip(nxs, nys, nzs)]
 
 
-def config4(seed: int = 20261203, n_domains: int = 64, shapes=None) -> List[RediProblem]:
-    """Uneven-domain batch: each domain seeded as config 0 with its own seamounts and mask."""
+def config4_domain(seed: int, d: int, shape) -> RediProblem:
+    """Domain d of the uneven-domain batch: seeded as config 0 with its own seamounts and mask."""
+    a, b, c = shape
+    return make_problem(a, b, c, n_seamounts=6, land_fraction=0.15, n_passive=4, seed=seed + 1 + d,
+                        name=f"config4_d{d}_{a}x{b}x{c}")
+
+
+def _config4_job(job):
+    return config4_domain(*job)
+
+
+def config4(seed: int = 20261203, n_domains: int = 64, shapes=None, workers: int = 1) -> List[RediProblem]:
+    """Uneven-domain batch: 64 domains, T, S and 4 passive tracers each.
+
+    ``workers`` > 1 generates the domains in a pool of spawned processes (the
+    result does not depend on it).
+    """
     shapes = shapes or config4_shapes(seed, n_domains)
-    return [make_problem(a, b, c, n_seamounts=6, land_fraction=0.15, n_passive=4, seed=seed + 1 + d,
-                         name=f"config4_d{d}_{a}x{b}x{c}") for d, (a, b, c) in enumerate(shapes)]
+    jobs = [(seed, d, s) for d, s in enumerate(shapes)]
+    if workers <= 1:
+        return [_config4_job(j) for j in jobs]
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    # largest first so the pool's tail is short; results returned in domain order
+    order = sorted(range(len(jobs)), key=lambda i: -jobs[i][2][0] * jobs[i][2][1] * jobs[i][2][2])
+    out: List[Optional[RediProblem]] = [None] * len(jobs)
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        for i, p in zip(order, ex.map(_config4_job, [jobs[i] for i in order])):
+            out[i] = p
+    return out
 
 
 def reference_ic(nx_phys: int = 473, ny_phys: int = 297, nz: int = 30) -> RediProblem:

@@ -416,3 +416,139 @@ def step(dp: DeviceProblem, redi: OceanRedi, nsteps: int = 1, stream=None) -> No
     for _ in range(nsteps):
         redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, stream)
         redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, stream)
+
+
+# ---------------------------------------------------------------------------
+# Many domains in one persistent launch (no counterpart in the reference)
+# ---------------------------------------------------------------------------
+STATUS_TIMEOUT = 1
+STAGE_NAMES = ("column_state", "neutral_sweep", "tracer_recon")
+
+
+class _Domain(C.Structure):
+    _fields_ = [("grid", _Grid), ("metrics", _Metrics), ("eos", _Eos), ("ms", _State),
+                ("khtr_u_ext", C.c_void_p), ("khtr_v_ext", C.c_void_p), ("bc", _BC), ("dt", C.c_double)]
+
+
+def _batch_lib() -> C.CDLL:
+    L = lib()
+    if not getattr(L, "_batch_types", False):
+        vp = C.c_void_p
+        L.redi_b200_batch_create.argtypes = [C.c_int, C.POINTER(_Domain), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                             C.POINTER(vp)]
+        L.redi_b200_batch_step.argtypes = [vp, vp]
+        L.redi_b200_batch_status.argtypes = [vp, _ip, _ip, _ip, _ip]
+        L.redi_b200_batch_set_wait_limit.argtypes = [vp, C.c_longlong]
+        L.redi_b200_batch_hold.argtypes = [vp, C.c_int, C.c_int]
+        L.redi_b200_batch_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.redi_b200_batch_get_tuning.argtypes = [vp, _ip, _ip, _ip, _ip, _ip]
+        L.redi_b200_batch_set_accounting.argtypes = [vp, C.c_int]
+        L.redi_b200_batch_stage_times.argtypes = [vp, _dp, _dp, C.POINTER(C.c_longlong)]
+        L.redi_b200_batch_updates.argtypes = [vp]
+        L.redi_b200_batch_updates.restype = C.c_longlong
+        L.redi_b200_batch_items.argtypes = [vp]
+        L.redi_b200_batch_items.restype = C.c_longlong
+        L.redi_b200_batch_destroy.argtypes = [vp]
+        L._batch_types = True
+    return L
+
+
+def stage_name(stage: int) -> str:
+    """Name of a stage index reported by ``RediBatch.status``."""
+    if stage < 3:
+        return STAGE_NAMES[stage]
+    g, kind = divmod(stage - 3, 2)
+    return f"{'face_flux' if kind == 0 else 'cell_gather'}[pair {g}]"
+
+
+class RediBatch:
+    """Independent regional domains stepped together by one persistent kernel.
+
+    ``domains`` are ``DeviceProblem``s (per-face diffusivities required); their
+    tensors must stay alive while the batch exists, their device addresses are
+    baked into it. Each ``step`` runs ``redi_calc_coeffs`` + ``redi_apply_flux``
+    on every domain; per domain the result equals the handle API's at the same
+    precision, bit for bit.
+    """
+
+    def __init__(self, domains: Sequence[DeviceProblem], precision: int = FP64, tile=(32, 4), chunk: int = 8,
+                 use_graph: bool = True):
+        L = _batch_lib()
+        self.domains = list(domains)
+        self.precision = precision
+        self.tile = tuple(tile)
+        self.chunk = chunk
+        self.use_graph = bool(use_graph)
+        arr = (_Domain * len(self.domains))()
+        keep = []
+        for k, dp in enumerate(self.domains):
+            st, tr = dp.ms._c()
+            keep.append(tr)
+            arr[k] = _Domain(dp.grid._c(), dp.metrics._c(), dp.eos._c(), st, _ptr(dp.khtr_u_ext), _ptr(dp.khtr_v_ext),
+                             dp.bc._c(), float(dp.dt))
+        h = C.c_void_p()
+        _check(L.redi_b200_batch_create(len(self.domains), arr, precision, int(tile[0]), int(tile[1]), int(chunk),
+                                        int(self.use_graph), C.byref(h)))
+        self._h = h
+
+    def step(self, nsteps: int = 1, stream=None) -> None:
+        s = _stream(stream)
+        for _ in range(nsteps):
+            _check(_batch_lib().redi_b200_batch_step(self._h, s))
+
+    def status(self) -> dict:
+        """Outcome of the last step (synchronises)."""
+        st, d, sg, bad = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(_batch_lib().redi_b200_batch_status(self._h, C.byref(st), C.byref(d), C.byref(sg), C.byref(bad)))
+        out = {"status": st.value, "bad": bad.value}
+        if st.value:
+            out.update(domain=d.value, stage=sg.value, stage_name=stage_name(sg.value))
+        return out
+
+    def set_wait_limit(self, ns: int) -> None:
+        _check(_batch_lib().redi_b200_batch_set_wait_limit(self._h, int(ns)))
+
+    def set_tuning(self, tile, chunk: int, occupancy: int = 0) -> None:
+        """Gather tile (bx, by), bx * by = 128, vertical chunk (4, 8, 16) and register budget
+        (blocks per SM: 4, 5, 6; 0 keeps it); results do not depend on it."""
+        _check(_batch_lib().redi_b200_batch_set_tuning(self._h, int(tile[0]), int(tile[1]), int(chunk),
+                                                       int(occupancy)))
+        self.tile, self.chunk = tuple(tile), chunk
+
+    def get_tuning(self) -> dict:
+        bx, by, ch, occ, grid = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(_batch_lib().redi_b200_batch_get_tuning(self._h, C.byref(bx), C.byref(by), C.byref(ch), C.byref(occ),
+                                                       C.byref(grid)))
+        return {"tile": (bx.value, by.value), "chunk": ch.value, "occupancy": occ.value, "grid": grid.value}
+
+    def set_accounting(self, on: bool = True) -> None:
+        _check(_batch_lib().redi_b200_batch_set_accounting(self._h, int(bool(on))))
+
+    def stage_times(self) -> dict:
+        """Per stage kind of the last step (accounting on): wait / busy ms summed over blocks, tiles."""
+        w, b, t = (C.c_double * 5)(), (C.c_double * 5)(), (C.c_longlong * 5)()
+        _check(_batch_lib().redi_b200_batch_stage_times(self._h, w, b, t))
+        names = ("column_state", "neutral_sweep", "tracer_recon", "face_flux", "cell_gather")
+        return {n: {"wait_ms": w[k], "busy_ms": b[k], "tiles": t[k]} for k, n in enumerate(names)}
+
+    def hold(self, domain: int, hold: bool = True) -> None:
+        _check(_batch_lib().redi_b200_batch_hold(self._h, int(domain), int(bool(hold))))
+
+    @property
+    def updates(self) -> int:
+        return int(_batch_lib().redi_b200_batch_updates(self._h))
+
+    @property
+    def items(self) -> int:
+        return int(_batch_lib().redi_b200_batch_items(self._h))
+
+    def destroy(self) -> None:
+        if getattr(self, "_h", None):
+            _batch_lib().redi_b200_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:  # pragma: no cover - interpreter shutdown
+            pass
