@@ -109,8 +109,8 @@ def kernel_bytes(p, kid: int, precision: str = "fp64") -> float:
         return 8.0 * s["Nt"] * (1 + s["ntr"])
     if kid in (4, 6):  # face flux: read the coefficients once for every tracer
         return float(bcoef + face2d)
-    if kid == 3:       # cell gather: read + write every tracer
-        return float(16 * s["Nt"] * s["ntr"] + 8 * s["ncol"])
+    if kid == 3:       # cell gather, one launch per tracer pair: read + write its tracers
+        return float(16 * s["Nt"] * min(2, s["ntr"]) + 8 * s["ncol"])
     return 0.0
 
 
@@ -310,11 +310,15 @@ def run_b200(args, rank, world, local_rank):
         from more_benchmarks_dc_ocean_b200 import autotune
 
         tuning = autotune.tune(dp, redi, use_cache=False, stream=st)
+        if p.ntr > 2:
+            tuning["tracer_group"] = autotune.tune_tracer_group(dp, redi, stream=st)
         if dist is not None:  # every rank uses rank 0's choice
-            t = torch.tensor(list(tuning["best"]), dtype=torch.int64, device=dev)
+            t = torch.tensor(list(tuning["best"]) + [autotune.get_tracer_group()], dtype=torch.int64, device=dev)
             dist.broadcast(t, 0)
-            autotune.set_tuning(*[int(v) for v in t.tolist()])
-            tuning["best"] = tuple(int(v) for v in t.tolist())
+            v = [int(x) for x in t.tolist()]
+            autotune.set_tuning(*v[:3])
+            autotune.set_tracer_group(v[3])
+            tuning["best"] = tuple(v[:3])
     L = R.lib()
     L.redi_b200_launch_count.restype = C.c_ulonglong
     L.redi_b200_launch_count.argtypes = [C.c_int]
@@ -393,6 +397,7 @@ def run_b200(args, rank, world, local_rank):
             "clocks": clk,
             "gpu_launches": int(n1 - n0),
             "tuning": {"cell_update_tile": list(tuning["best"][:2]), "vertical_chunk": tuning["best"][2],
+                       "tracer_group": tuning.get("tracer_group"),
                        "candidates_ms": tuning["ms"]} if tuning else None,
             "hbm_gbs_per_rank": bstep / (ms_all * 1e-3) / 1e9,
         }
@@ -435,7 +440,7 @@ def run_domains(args, rank, world, local_rank):
     # Inputs are generated before the first GPU call (the pool is spawned).
     workers = max(1, min(len(os.sched_getaffinity(0)), 16))
     t_gen = time.perf_counter()
-    ps = inputs.config4(seed=20261203 + 1000 * rank, workers=workers)
+    ps = inputs.config4(seed=20261203 + 1000 * rank, n_domains=args.domains, workers=workers)
     t_gen = time.perf_counter() - t_gen
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -718,6 +723,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--domains", type=int, default=64, help="config4: number of regional domains")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

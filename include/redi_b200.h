@@ -172,6 +172,13 @@ REDI_B200_API int redi_b200_kernel_count(void);
  * (4, 8 or 16). Results do not depend on it; the autotuner picks it. */
 REDI_B200_API int redi_b200_set_tuning(int bx, int by, int chunk);
 REDI_B200_API int redi_b200_get_tuning(int* bx, int* by, int* chunk);
+
+/* Largest number of tracers whose face fluxes one launch computes (1, 2, 4
+ * or 8; default 8), process-wide (no counterpart in the reference). Larger
+ * groups read the Phase-A coefficients fewer times per step, smaller ones run
+ * at higher occupancy; results do not depend on it. */
+REDI_B200_API int redi_b200_set_tracer_group(int max_group);
+REDI_B200_API int redi_b200_get_tracer_group(void);
 REDI_B200_API unsigned long long redi_b200_launch_count(int kernel);
 REDI_B200_API int redi_b200_profile_begin(void);
 REDI_B200_API int redi_b200_profile_end(double* total_ms, unsigned long long* counts, int n);

@@ -50,6 +50,49 @@ def set_tuning(bx: int, by: int, chunk: int) -> None:
     R._check(_bind(R.lib()).redi_b200_set_tuning(int(bx), int(by), int(chunk)))
 
 
+def set_tracer_group(max_group: int) -> None:
+    """Largest tracer group of one face-flux launch (1, 2, 4, 8)."""
+    from . import ocean_redi as R
+
+    L = R.lib()
+    L.redi_b200_set_tracer_group.argtypes = [C.c_int]
+    R._check(L.redi_b200_set_tracer_group(int(max_group)))
+
+
+def get_tracer_group() -> int:
+    from . import ocean_redi as R
+
+    return int(R.lib().redi_b200_get_tracer_group())
+
+
+def tune_tracer_group(dp, redi, reps: int = 2, stream=None) -> dict:
+    """Time redi_apply_flux for every tracer-group cap the tracer count allows; keep the fastest.
+
+    Advances dp's tracers in place. Returns {"best": cap, "ms": {cap: ms per apply_flux}}.
+    """
+    import torch
+
+    from . import ocean_redi as R
+
+    ntr = len(dp.ms.tracers)
+    caps = [g for g in (2, 4, 8) if g <= max(2, ntr)]
+    st = torch.cuda.current_stream() if stream is None else stream
+    times = {}
+    for g in caps:
+        set_tracer_group(g)
+        R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, st)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, st)
+        e1.record(st)
+        torch.cuda.synchronize()
+        times[g] = e0.elapsed_time(e1) / reps
+    best = min(times, key=times.get)
+    set_tracer_group(best)
+    return {"best": best, "ms": {str(g): round(v, 4) for g, v in times.items()}}
+
+
 def _key(dp, precision: int) -> str:
     import torch
 

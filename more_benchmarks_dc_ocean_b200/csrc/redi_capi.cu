@@ -146,13 +146,14 @@ template <class P>
 int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch& ws, cudaStream_t st) {
     const int batch = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
     const size_t recon = redi::recon_bytes<P>(in.nx, in.ny, in.nz, batch);
-    const size_t flux = redi::flux_bytes<P>(in.nx, in.ny, in.nz, redi::tracer_group(batch));
+    const int group = redi::tracer_group(batch, redi::cell_tuning().group);
+    const size_t flux = redi::flux_bytes<P>(in.nx, in.ny, in.nz, group);
     cudaError_t e = ws.reserve(recon + flux);
     if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (phase B)");
     const size_t ns1 = (size_t)(2 * in.nz + 1);
     using Flux = typename P::Flux;
     Flux* Fu = reinterpret_cast<Flux*>(static_cast<char*>(ws.data()) + recon);
-    Flux* Fv = Fu + (size_t)redi::tracer_group(batch) * ns1 * (size_t)(in.nx + 1) * in.ny;
+    Flux* Fv = Fu + (size_t)group * ns1 * (size_t)(in.nx + 1) * in.ny;
     for (int t0 = 0; t0 < ntr; t0 += batch) {
         const int nt = (ntr - t0) < batch ? (ntr - t0) : batch;
         redi::ReconArgsT<P> rc{};
@@ -206,7 +207,7 @@ Profiler g_prof;
 namespace redi {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-static CellTuning g_cell_tuning{32, 4, 8};
+static CellTuning g_cell_tuning{32, 4, 8, 8};
 CellTuning cell_tuning() { return g_cell_tuning; }
 void set_cell_tuning(const CellTuning& t) { g_cell_tuning = t; }
 
@@ -295,9 +296,20 @@ int redi_b200_set_tuning(int bx, int by, int chunk) {
         return fail(REDI_B200_E_ARG, "redi_b200_set_tuning: bx*by must be a multiple of 32 and at most 128");
     if (chunk != 4 && chunk != 8 && chunk != 16)
         return fail(REDI_B200_E_ARG, "redi_b200_set_tuning: chunk must be 4, 8 or 16");
-    redi::set_cell_tuning(redi::CellTuning{bx, by, chunk});
+    redi::set_cell_tuning(redi::CellTuning{bx, by, chunk, redi::cell_tuning().group});
     return REDI_B200_OK;
 }
+
+int redi_b200_set_tracer_group(int max_group) {
+    if (max_group != 1 && max_group != 2 && max_group != 4 && max_group != 8)
+        return fail(REDI_B200_E_ARG, "redi_b200_set_tracer_group: max_group must be 1, 2, 4 or 8");
+    redi::CellTuning t = redi::cell_tuning();
+    t.group = max_group;
+    redi::set_cell_tuning(t);
+    return REDI_B200_OK;
+}
+
+int redi_b200_get_tracer_group(void) { return redi::cell_tuning().group; }
 
 int redi_b200_get_tuning(int* bx, int* by, int* chunk) {
     if (!bx || !by || !chunk) return fail(REDI_B200_E_ARG, "redi_b200_get_tuning: NULL argument");

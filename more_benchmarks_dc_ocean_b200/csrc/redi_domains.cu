@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(kThreads, OCC) k_domains(const DomainDev<P>* _
                 const int by = kThreads / bx;
                 const int i = (it.tile % d.gx) * bx + tid % bx;
                 const int j = (it.tile / d.gx) * by + tid / bx;
-                plain::gather_item<2, CH, P, LdCG>(d.cg, i, j, 2 * pair);
+                plain::gather_item<2, CH, P, LdCG>(d.cg, i, j, 2 * pair, 0);
             }
         }
         __syncthreads();

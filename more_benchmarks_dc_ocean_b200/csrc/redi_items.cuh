@@ -416,28 +416,35 @@ __device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double interp(double P, double a, double b) { return (1.0 - P) * a + P * b; }
 
-// Layer mean of the PPM parabola and the flux product, per precision.
+// Layer mean of the PPM parabola and the flux product, per precision. `load`
+// fetches a prepared layer, `mean` evaluates it (split so that every load of a
+// sublayer can be issued before any of them is used).
 template <class P>
 struct FluxOps;
 
 template <>
 struct FluxOps<PlainPrec> {
     using Mean = double;
+    using Raw = PpmLayer;
     template <class LD>
-    __device__ static __forceinline__ double mean(double xL, double xR, const PpmLayer* p) {
-        return ppm_ave(xL, xR, load_ppm<LD>(p));
+    __device__ static __forceinline__ Raw load(const PpmLayer* p) {
+        return load_ppm<LD>(p);
     }
+    __device__ static __forceinline__ double mean(double xL, double xR, const Raw& q) { return ppm_ave(xL, xR, q); }
     __device__ static __forceinline__ double flux(double dT, double he, double coef) { return dT * he * coef; }
 };
 
 template <>
 struct FluxOps<MixedPrec> {
     using Mean = float;
+    using Raw = float4;  // aL, dA, a6o3, B
+    template <class LD>
+    __device__ static __forceinline__ Raw load(const PpmLayerF* p) {
+        return LD::ld(reinterpret_cast<const float4*>(p));
+    }
     // redi_ppm_ave in FP32; the branch (a discrete decision) is taken on the
     // FP64 positions exactly as in the plain form.
-    template <class LD>
-    __device__ static __forceinline__ float mean(double xL, double xR, const PpmLayerF* p) {
-        const float4 q = LD::ld(reinterpret_cast<const float4*>(p));  // aL, dA, a6o3, B
+    __device__ static __forceinline__ float mean(double xL, double xR, const Raw& q) {
         const float xl = (float)xL, xr = (float)xR;
         const double dx = xR - xL;
         if (dx > 0.0 && dx <= 1.0) {
@@ -452,34 +459,50 @@ struct FluxOps<MixedPrec> {
     }
 };
 
+// Every lane of the warp must call this (no lane may have exited): lanes
+// without a face of their own (grid tail, wall faces) walk face 0 of their
+// direction as a stand-in, load like the others and store nothing, so the
+// warp-wide vote below is well defined. A warp whose every lane has
+// hEff == 0 at a sublayer (land, outcropped layers) skips that sublayer's
+// loads; otherwise the whole warp issues a pair of tracers' loads for the
+// sublayer (bottom surface tracer values, PPM layers, and top values after a
+// skip) as one batch before any of them is used, so each sublayer costs one
+// memory round trip per tracer pair.
 template <int NT, class P, class LD>
 __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, int t, int tr0) {
     using Ops = FluxOps<P>;
+    using Raw = typename Ops::Raw;
+    using He = typename P::He;
     const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
     const size_t ncol = (size_t)nx * ny;
     int colL, colR, fo;
     size_t fstride;
+    bool valid;
+    if ((dir == 0 ? (nx - 1) * ny : nx * (ny - 1)) <= 0) return;  // no face 0 to stand in
     if (dir == 0) {  // Fortran faces I = 2..nx, excluding walls
-        if (t >= (nx - 1) * ny) return;
-        const int j = t / (nx - 1), fi = 1 + t % (nx - 1);
+        valid = t < (nx - 1) * ny;
+        const int tt = valid ? t : 0;
+        const int j = tt / (nx - 1), fi = 1 + tt % (nx - 1);
         const int I = fi + 1;
-        if ((a.wall_w && I == a.nghost + 1) || (a.wall_e && I == a.nghost + a.nxp + 1)) return;
+        valid = valid && !((a.wall_w && I == a.nghost + 1) || (a.wall_e && I == a.nghost + a.nxp + 1));
         colL = (fi - 1) + nx * j;
         colR = fi + nx * j;
         fo = fi + (nx + 1) * j;
         fstride = (size_t)(nx + 1) * ny;
     } else {  // Fortran faces J = 2..ny, excluding walls
-        if (t >= nx * (ny - 1)) return;
-        const int fj = 1 + t / nx, i = t % nx;
+        valid = t < nx * (ny - 1);
+        const int tt = valid ? t : 0;
+        const int fj = 1 + tt / nx, i = tt % nx;
         const int J = fj + 1;
-        if ((a.wall_s && J == a.nghost + 1) || (a.wall_n && J == a.nghost + a.nyp + 1)) return;
+        valid = valid && !((a.wall_s && J == a.nghost + 1) || (a.wall_n && J == a.nghost + a.nyp + 1));
         colL = i + nx * (fj - 1);
         colR = i + nx * fj;
         fo = i + nx * fj;
         fstride = (size_t)nx * (ny + 1);
     }
+    if (!__any_sync(0xffffffffu, valid)) return;  // warp-uniform
     const FaceInT<P>& c = dir == 0 ? a.u : a.v;
-    const typename P::He* __restrict__ hEff = c.hEff + fo;
+    const He* __restrict__ hEff = c.hEff + fo;
     const typename P::Po* __restrict__ PoL = c.PoL + fo;
     const typename P::Po* __restrict__ PoR = c.PoR + fo;
     const typename P::Ko* __restrict__ KoL = c.KoL + fo;
@@ -490,26 +513,21 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
     const double coef = a.dt * khv * LD::ld((dir == 0 ? a.dy_cu : a.dx_cv) + fo) *
                         LD::ld((dir == 0 ? a.idxCu : a.idyCv) + fo);
     const int nt = min(NT, a.ntr - tr0);
-    const double* tiL[NT];
-    const double* tiR[NT];
-    const typename P::Ppm* ppL[NT];
-    const typename P::Ppm* ppR[NT];
-    typename P::Flux* Fo[NT];
-#pragma unroll
-    for (int n = 0; n < NT; ++n) {
-        const int tr = tr0 + (n < nt ? n : 0);
-        tiL[n] = a.ti + (size_t)tr * ncol * (nz + 1) + colL;
-        tiR[n] = a.ti + (size_t)tr * ncol * (nz + 1) + colR;
-        ppL[n] = a.ppm + (size_t)tr * ncol * nz + colL;
-        ppR[n] = a.ppm + (size_t)tr * ncol * nz + colR;
-        Fo[n] = (dir == 0 ? a.Fu : a.Fv) + (size_t)(tr - tr0) * (size_t)(ns - 1) * fstride + fo;
-    }
+    // Tracers of the group sit at fixed strides in the scratch; a tracer slot
+    // beyond nt reads tracer tr0 and stores nothing.
+    const size_t ti_stride = ncol * (nz + 1), pp_stride = ncol * nz, f_stride = (size_t)(ns - 1) * fstride;
+    const double* const tiL0 = a.ti + (size_t)tr0 * ti_stride + colL;
+    const double* const tiR0 = a.ti + (size_t)tr0 * ti_stride + colR;
+    const typename P::Ppm* const ppL0 = a.ppm + (size_t)tr0 * pp_stride + colL;
+    const typename P::Ppm* const ppR0 = a.ppm + (size_t)tr0 * pp_stride + colR;
+    typename P::Flux* const Fo0 = (dir == 0 ? a.Fu : a.Fv) + fo;
+    auto trc = [nt](int n) { return (size_t)(n < nt ? n : 0); };
 
     // Register rotation: while sublayer s is evaluated, hEff(s+1) and the
     // bottom surface of s+1 (surface s+2) are already being fetched. The top
-    // surface of s is always the bottom surface of s-1.
-    using He = typename P::He;
-    bool have_t = false;  // tl/tr hold the tracer values at the top surface
+    // surface of s is the bottom surface of s-1 (tl/tr carry its tracer
+    // values unless the previous sublayer was skipped by the whole warp).
+    bool have_t = false;  // warp-uniform
     int kl_t = min(max((int)LD::ld(KoL), 1), nz), kr_t = min(max((int)LD::ld(KoR), 1), nz);
     double pl_t = LD::ld(PoL), pr_t = LD::ld(PoR);
     He he_c = LD::ld(hEff);
@@ -532,33 +550,59 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
         const int kl_b = min(max(klr_c, 1), nz);
         const int kr_b = min(max(krr_c, 1), nz);
         const double pl_b = pl_c, pr_b = pr_c;
-        if (he_c == He(0)) {
+        const bool live = valid && he_c != He(0);
+        if (!__any_sync(0xffffffffu, live)) {
 #pragma unroll
             for (int n = 0; n < NT; ++n)
-                if (n < nt) Fo[n][s0] = typename P::Flux(0);
+                if (valid && n < nt) Fo0[(size_t)n * f_stride + s0] = typename P::Flux(0);
             have_t = false;
         } else {
-            if (!have_t) {
-#pragma unroll
-                for (int n = 0; n < NT; ++n) {
-                    tl[n] = interp(pl_t, LD::ld(tiL[n] + (size_t)(kl_t - 1) * ncol), LD::ld(tiL[n] + (size_t)kl_t * ncol));
-                    tr[n] = interp(pr_t, LD::ld(tiR[n] + (size_t)(kr_t - 1) * ncol), LD::ld(tiR[n] + (size_t)kr_t * ncol));
-                }
-            }
             const double xRl = pl_b + (double)(kl_b - kl_t);
             const double xRr = pr_b + (double)(kr_b - kr_t);
+            // Tracers in pairs, one load batch per pair: bottom-surface tracer
+            // values and the top layer's PPM, then (after a skip) the
+            // top-surface values; the compiler barrier keeps the next pair's
+            // loads from being hoisted into this batch (register budget).
 #pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                const double bl = interp(pl_b, LD::ld(tiL[n] + (size_t)(kl_b - 1) * ncol), LD::ld(tiL[n] + (size_t)kl_b * ncol));
-                const double br = interp(pr_b, LD::ld(tiR[n] + (size_t)(kr_b - 1) * ncol), LD::ld(tiR[n] + (size_t)kr_b * ncol));
-                if (n < nt) {
-                    const typename Ops::Mean tlay = Ops::template mean<LD>(pl_t, xRl, ppL[n] + (size_t)(kl_t - 1) * ncol);
-                    const typename Ops::Mean trlay = Ops::template mean<LD>(pr_t, xRr, ppR[n] + (size_t)(kr_t - 1) * ncol);
-                    const double dT = guarded_dT(tr[n] - tl[n], br - bl, (double)(trlay - tlay));
-                    Fo[n][s0] = Ops::flux(dT, he_c, coef);
+            for (int p = 0; p < NT; p += 2) {
+                constexpr int W = NT < 2 ? NT : 2;
+                double b0L[W], b1L[W], b0R[W], b1R[W];
+                Raw qL[W], qR[W];
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    const int n = p + w;
+                    b0L[w] = LD::ld(tiL0 + trc(n) * ti_stride + (size_t)(kl_b - 1) * ncol);
+                    b1L[w] = LD::ld(tiL0 + trc(n) * ti_stride + (size_t)kl_b * ncol);
+                    b0R[w] = LD::ld(tiR0 + trc(n) * ti_stride + (size_t)(kr_b - 1) * ncol);
+                    b1R[w] = LD::ld(tiR0 + trc(n) * ti_stride + (size_t)kr_b * ncol);
+                    qL[w] = Ops::template load<LD>(ppL0 + trc(n) * pp_stride + (size_t)(kl_t - 1) * ncol);
+                    qR[w] = Ops::template load<LD>(ppR0 + trc(n) * pp_stride + (size_t)(kr_t - 1) * ncol);
                 }
-                tl[n] = bl;
-                tr[n] = br;
+                if (!have_t) {
+#pragma unroll
+                    for (int w = 0; w < W; ++w) {
+                        const int n = p + w;
+                        tl[n] = interp(pl_t, LD::ld(tiL0 + trc(n) * ti_stride + (size_t)(kl_t - 1) * ncol),
+                                       LD::ld(tiL0 + trc(n) * ti_stride + (size_t)kl_t * ncol));
+                        tr[n] = interp(pr_t, LD::ld(tiR0 + trc(n) * ti_stride + (size_t)(kr_t - 1) * ncol),
+                                       LD::ld(tiR0 + trc(n) * ti_stride + (size_t)kr_t * ncol));
+                    }
+                }
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    const int n = p + w;
+                    const double bl = interp(pl_b, b0L[w], b1L[w]);
+                    const double br = interp(pr_b, b0R[w], b1R[w]);
+                    if (valid && n < nt) {
+                        const typename Ops::Mean tlay = Ops::mean(pl_t, xRl, qL[w]);
+                        const typename Ops::Mean trlay = Ops::mean(pr_t, xRr, qR[w]);
+                        const double dT = guarded_dT(tr[n] - tl[n], br - bl, (double)(trlay - tlay));
+                        Fo0[(size_t)n * f_stride + s0] = he_c == He(0) ? typename P::Flux(0) : Ops::flux(dT, he_c, coef);
+                    }
+                    tl[n] = bl;
+                    tr[n] = br;
+                }
+                if (p + 2 < NT) asm volatile("" ::: "memory");
             }
             have_t = true;
         }
@@ -600,13 +644,11 @@ __device__ __forceinline__ void gather_run(const typename P::Flux* const (&F)[NT
                                            const typename P::Ko* __restrict__ KoS, size_t stride, bool left, int ns,
                                            int& ptr, int k0, int k1, double (&dTr)[NT][CH], int& bad) {
     // Sublayers are fetched U at a time (independent loads in flight), then
-    // consumed in order until the first one beyond the chunk.
+    // consumed in order until the first one beyond the chunk. The per-layer
+    // sums stay in registers (see below).
     constexpr int U = 4;
-    int cur = -1;
-    double acc[NT];
     int s = ptr;
-    bool done = false;
-    while (!done && s < ns - 1) {
+    while (s < ns - 1) {
         int kk[U];
         double ff[U][NT];
 #pragma unroll
@@ -623,41 +665,38 @@ __device__ __forceinline__ void gather_run(const typename P::Flux* const (&F)[NT
                 for (int n = 0; n < NT; ++n) ff[u][n] = 0.0;
             }
         }
+        bool stop = false;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            if (done) break;
             const int k = kk[u];
-            if (k >= k1) {  // also the end of the face (s >= ns-1)
-                done = true;
-                break;
-            }
-            ++s;
-            if (k < k0) {
-                ++bad;
-                continue;
-            }
-            const int slot = k - k0;
-            if (slot != cur) {
+            stop = stop || k >= k1;  // also the end of the face (s >= ns-1)
+            if (!stop) {
+                ++s;
+                if (k < k0) ++bad;
+                // Every slot takes a term: the flux where the index matches,
+                // +0.0 elsewhere, which leaves the slot unchanged (it is never
+                // -0.0) -- the same additions in the same order as an indexed
+                // update, without a dynamically indexed array.
 #pragma unroll
-                for (int n = 0; n < NT; ++n) {
-                    if (cur >= 0) dTr[n][cur] = acc[n];
-                    acc[n] = dTr[n][slot];
+                for (int c = 0; c < CH; ++c) {
+                    const bool hit = k - k0 == c;
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) {
+                        const double f = hit ? ff[u][n] : 0.0;
+                        dTr[n][c] = left ? dTr[n][c] + f : dTr[n][c] - f;
+                    }
                 }
-                cur = slot;
             }
-#pragma unroll
-            for (int n = 0; n < NT; ++n) acc[n] = left ? acc[n] + ff[u][n] : acc[n] - ff[u][n];
         }
+        if (stop) break;
     }
     ptr = s;
-    if (cur >= 0) {
-#pragma unroll
-        for (int n = 0; n < NT; ++n) dTr[n][cur] = acc[n];
-    }
 }
 
 template <int NT, int CH, class P, class LD>
-__device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, int j, int tr0) {
+// Tracers tr0 .. tr0+NT-1 of the state; their fluxes sit at slots
+// fslot .. fslot+NT-1 of the flux buffer.
+__device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, int j, int tr0, int fslot) {
     const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
     if (i >= nx || j >= ny) return;
     const size_t ncol = (size_t)nx * ny;
@@ -692,7 +731,7 @@ __device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, 
             const typename P::Flux* F[NT];
 #pragma unroll
             for (int n = 0; n < NT; ++n)
-                F[n] = (u ? a.Fu : a.Fv) + (size_t)(n < nt ? n : 0) * (size_t)(ns - 1) * stride + fo[f];
+                F[n] = (u ? a.Fu : a.Fv) + (size_t)(fslot + (n < nt ? n : 0)) * (size_t)(ns - 1) * stride + fo[f];
             const FaceInT<P>& c = u ? a.u : a.v;
             gather_run<NT, CH, P, LD>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1, dTr, bad);
         }

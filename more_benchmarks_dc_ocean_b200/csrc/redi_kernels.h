@@ -153,8 +153,13 @@ inline size_t flux_bytes(int nx, int ny, int nz, int group) {
     const size_t faces = (size_t)(nx + 1) * ny + (size_t)nx * (ny + 1);
     return (size_t)group * (size_t)(2 * nz + 1) * faces * sizeof(typename P::Flux);
 }
-// Tracers per face-flux / gather launch for a set of ntr tracers.
-inline int tracer_group(int ntr) { return ntr >= 8 ? 8 : ntr >= 4 ? 4 : ntr >= 2 ? 2 : 1; }
+// Tracers per face-flux launch for a set of ntr tracers, at most cap (1, 2,
+// 4 or 8): a larger group reads the coefficients fewer times, a smaller one
+// needs fewer registers.
+inline int tracer_group(int ntr, int cap = 8) {
+    const int g = ntr >= 8 ? 8 : ntr >= 4 ? 4 : ntr >= 2 ? 2 : 1;
+    return g < cap ? g : cap;
+}
 
 // Kernel identities for the launch counter and the optional event timing.
 enum KernelId : int {
@@ -180,10 +185,11 @@ void set_last_error(const std::string& msg);
 void launch_begin(int kid, cudaStream_t st);
 void launch_end(int kid, cudaStream_t st);
 
-// Launch shape of the cell gather: a bx x by tile of columns per block
-// (bx * by <= 128) and the vertical chunk (layers per pass, 4, 8 or 16).
+// Launch shape of Phase B: the cell gather's bx x by tile of columns per
+// block (bx * by <= 128) and vertical chunk (layers per pass, 4, 8 or 16),
+// and the largest tracer group of one face-flux launch (1, 2, 4 or 8).
 struct CellTuning {
-    int bx, by, chunk;
+    int bx, by, chunk, group;
 };
 CellTuning cell_tuning();
 void set_cell_tuning(const CellTuning& t);

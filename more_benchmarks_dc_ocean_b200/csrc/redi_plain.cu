@@ -65,9 +65,9 @@ __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0) 
 }
 
 template <int NT, int CH, class P>
-__global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgsT<P> a, int tr0) {
+__global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgsT<P> a, int tr0, int fslot) {
     gather_item<NT, CH, P, LdNC>(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y,
-                                 tr0);
+                                 tr0, fslot);
 }
 
 }  // namespace plain
@@ -107,13 +107,18 @@ static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT
         plain::k_face_flux<NT, P><<<dim3((nface + 127) / 128, 2), 128, 0, st>>>(ff, tr0);
         launch_end(kid, st);
     }
-    launch_begin(K_CELL_UPDATE, st);
-    switch (tune.chunk) {
-        case 4: plain::k_cell_gather<NT, 4, P><<<cgrid, block, 0, st>>>(cg, tr0); break;
-        case 16: plain::k_cell_gather<NT, 16, P><<<cgrid, block, 0, st>>>(cg, tr0); break;
-        default: plain::k_cell_gather<NT, 8, P><<<cgrid, block, 0, st>>>(cg, tr0); break;
+    // The gather folds tracer pairs (its per-layer sums live in registers);
+    // a group's pairs read consecutive slots of the flux buffer.
+    for (int g = 0; g < NT; g += 2) {
+        if (tr0 + g >= cg.ntr) break;
+        launch_begin(K_CELL_UPDATE, st);
+        switch (tune.chunk) {
+            case 4: plain::k_cell_gather<NT < 2 ? NT : 2, 4, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g); break;
+            case 16: plain::k_cell_gather<NT < 2 ? NT : 2, 16, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g); break;
+            default: plain::k_cell_gather<NT < 2 ? NT : 2, 8, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g); break;
+        }
+        launch_end(K_CELL_UPDATE, st);
     }
-    launch_end(K_CELL_UPDATE, st);
 }
 
 template <class P>
@@ -131,7 +136,7 @@ cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, 
     }
     const CellTuning tune = cell_tuning();
     const int nface = max((ff.nx - 1) * ff.ny, ff.nx * (ff.ny - 1));
-    const int group = tracer_group(ff.ntr);
+    const int group = tracer_group(ff.ntr, tune.group);
     for (int tr0 = 0; tr0 < ff.ntr; tr0 += group) {
         switch (group) {
             case 8: launch_flux_gather<8, P>(ff, cg, tr0, nface, tune, st); break;
