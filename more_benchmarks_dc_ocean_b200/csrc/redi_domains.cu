@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(kThreads, OCC) k_domains(const DomainDev<P>* _
         } else if (st == S_SWEEP) {
             const int dir = it.tile < d.nu_tiles ? 0 : 1;
             const int t = (dir == 0 ? it.tile : it.tile - d.nu_tiles) * kThreads + tid;
-            plain::sweep_item<P, LdCG>(d.sw, dir, t);
+            plain::sweep_item<P, LdCG, false>(d.sw, dir, t);
         } else if (st == S_RECON) {
             plain::recon_item<2, P, LdCG>(d.rc, it.tile * kThreads + tid);
         } else {

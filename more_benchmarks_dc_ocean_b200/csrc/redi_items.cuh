@@ -19,29 +19,50 @@ namespace plain {
 // Streaming top-down PPM interface reconstruction (redi_interface_scalar,
 // ocean_redi.F90:231-254) of NS scalars that share one thickness column.
 //
-// Layers are pulled from the surface down through `load(t, h, s)`, t = 1..nk
-// top-down; edge(t) needs layers t-2..t+1, so a four-layer register window
-// replaces the reference's column arrays. `emit(t, e, s_above)` receives
-// interface t (1..nk+1), its NS edge values, and the NS means of the layer
-// just above it (layer t-1; undefined for t = 1).
+// Layers are pulled from the surface down, t = 1..nk top-down: `fetch(t, r)`
+// issues the raw loads of layer t (thickness and the NS thickness-weighted
+// scalars) into r; the layer's means (hTr / max(h, eps)) are formed one
+// iteration later, so every load has a full iteration to arrive. edge(t)
+// needs layers t-2..t+1, so a four-layer register window replaces the
+// reference's column arrays. `emit(t, e, s_above, h_t)` receives interface t
+// (1..nk+1), its NS edge values, the NS means of the layer just above it
+// (layer t-1; undefined for t = 1) and the thickness of layer t (t <= nk).
 // ---------------------------------------------------------------------------
-template <int NS, class Load, class Emit>
-__device__ __forceinline__ void stream_edges(int nk, Load load, Emit emit) {
+template <int NS>
+struct RawLayer {
+    double h;
+    double s[NS];
+};
+
+template <int NS>
+__device__ __forceinline__ void finish_layer(const RawLayer<NS>& r, double& hv, double (&sv)[NS]) {
+    const double he = fmax(r.h, kHDivEps);
+    hv = r.h;
+#pragma unroll
+    for (int n = 0; n < NS; ++n) sv[n] = r.s[n] / he;
+}
+
+template <int NS, class Fetch, class Emit>
+__device__ __forceinline__ void stream_edges(int nk, Fetch fetch, Emit emit) {
     double hA = 0.0, hB, hC, hD = 0.0;  // h(t-2), h(t-1), h(t), h(t+1)
     double sB[NS], sC[NS], sD[NS];      // layer scalars t-1, t, t+1
     double dB[NS], dC[NS];              // PLM slopes of layers t-1, t
     double e[NS];
+    RawLayer<NS> r1, r2, rn;            // rn: raw layer t+2, in flight
 
     // t = 1: edge(1) = tr(1) - 0.5*diff(1), diff(1) = 0.
-    load(1, hC, sC);
-    if (nk >= 2) load(2, hD, sD);
+    fetch(1, r1);
+    if (nk >= 2) fetch(2, r2);
+    if (nk >= 3) fetch(3, rn);
+    finish_layer(r1, hC, sC);
+    if (nk >= 2) finish_layer(r2, hD, sD);
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
         dC[n] = 0.0;
         e[n] = sC[n] - 0.5 * dC[n];
         sB[n] = 0.0;
     }
-    emit(1, e, sB);
+    emit(1, e, sB, hC);
 
     for (int t = 2; t <= nk; ++t) {
         // shift the window down one layer: (t-1) <- t, t <- t+1
@@ -54,7 +75,10 @@ __device__ __forceinline__ void stream_edges(int nk, Load load, Emit emit) {
             sC[n] = sD[n];
             dB[n] = dC[n];
         }
-        if (t + 1 <= nk) load(t + 1, hD, sD);
+        if (t + 1 <= nk) {
+            finish_layer(rn, hD, sD);
+            if (t + 2 <= nk) fetch(t + 2, rn);
+        }
         // diff(t): PLM slope for 2 <= t <= nk-1, PCM (0) at t = nk.
         if (t <= nk - 1) {
             const PlmGeom pg = plm_geom(hB, hC, hD);
@@ -69,12 +93,12 @@ __device__ __forceinline__ void stream_edges(int nk, Load load, Emit emit) {
         const EdgeGeom eg = edge_geom(hkm1, hB, hC, hkp2, kHNeglect);
 #pragma unroll
         for (int n = 0; n < NS; ++n) e[n] = ppm_edge(eg, sB[n], sC[n], dB[n], dC[n]);
-        emit(t, e, sB);
+        emit(t, e, sB, hC);
     }
     // edge(nk+1) = tr(nk) + 0.5*diff(nk), diff(nk) = 0.
 #pragma unroll
     for (int n = 0; n < NS; ++n) e[n] = sC[n] + 0.5 * dC[n];
-    emit(nk + 1, e, sC);
+    emit(nk + 1, e, sC, 0.0);
 }
 
 // ---------------------------------------------------------------------------
@@ -98,24 +122,22 @@ __device__ __forceinline__ void column_state_item(const ColumnStateArgs& a, int 
     double P = 0.0;
     double h_layer_above = 0.0;
 
-    auto load = [&](int t, double& hv, double (&sv)[2]) {
+    auto fetch = [&](int t, RawLayer<2>& r) {
         const size_t off = (size_t)(nz - t) * ncol;  // native k = nz+1-t (1-based)
-        const double hk = LD::ld(h + off);
-        const double he = fmax(hk, kHDivEps);
-        hv = hk;
-        sv[0] = LD::ld(th + off) / he;
-        sv[1] = LD::ld(sh + off) / he;
+        r.h = LD::ld(h + off);
+        r.s[0] = LD::ld(th + off);
+        r.s[1] = LD::ld(sh + off);
     };
-    auto emit = [&](int t, const double (&e)[2], const double (&)[2]) {
+    auto emit = [&](int t, const double (&e)[2], const double (&)[2], double h_t) {
         if (t >= 2) P = P + grho * h_layer_above;  // Pint(t) = Pint(t-1) + g*rho0*h(t-1)
         const double rho_i = eos.rho0 + eos.beta_S * (e[1] - eos.S_ref) - eos.alpha_T * (e[0] - eos.T_ref);
         double2* q = reinterpret_cast<double2*>(ifc + (size_t)(t - 1) * ncol);
         q[0] = make_double2(e[0], e[1]);
         q[1] = make_double2(-(rho_i * rho_i) * dsv_dt, -(rho_i * rho_i) * dsv_ds);
         pint[(size_t)(t - 1) * ncol] = P;
-        if (t <= nz) h_layer_above = LD::ld(h + (size_t)(nz - t) * ncol);
+        h_layer_above = h_t;
     };
-    stream_edges<2>(nz, load, emit);
+    stream_edges<2>(nz, fetch, emit);
 }
 
 // ---------------------------------------------------------------------------
@@ -136,11 +158,91 @@ struct ColWin {
     IfcState a, b, c;   // interfaces km1, km1+1, km1+2 (1-based)
     double pa, pb, pc;  // pressures at the same interfaces
     int k;              // the pointer (1-based, 1..nk+1)
+    int side;           // 0 left column, 1 right column (its ring)
 };
 
+// Look-ahead of the window: interfaces km1+3 and km1+4 of each column are in
+// flight into a per-thread ring in shared memory (cp.async), issued two shifts
+// before they enter the registers. A register window that loaded its next
+// interface straight into the slot it rotates from would make the rotation
+// itself wait on that load whenever one column advances on consecutive steps;
+// here registers only ever receive settled values. Blocks of 128 threads.
+constexpr int kSweepRing = 4;
+constexpr int kSweepThreads = 128;
+struct SweepRing {
+    IfcState x[kSweepRing][2][kSweepThreads];
+    double p[kSweepRing][2][kSweepThreads];
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Ring slot q (0-based interface index, taken mod the ring) <- interface
+// min(q, nk) of the column.
+__device__ __forceinline__ void ring_fetch(SweepRing& r, int side, int q, const IfcState* X, const double* P, int nk,
+                                           size_t ld) {
+    const int slot = q % kSweepRing, qi = min(q, nk), tid = threadIdx.x;
+    const IfcState* src = X + (size_t)qi * ld;
+    cp_async16(&r.x[slot][side][tid], src);
+    cp_async16(reinterpret_cast<char*>(&r.x[slot][side][tid]) + 16, reinterpret_cast<const char*>(src) + 16);
+    cp_async8(&r.p[slot][side][tid], P + (size_t)qi * ld);
+}
+
 template <class LD>
-__device__ __forceinline__ void win_init(ColWin& w, const IfcState* X, const double* P, int nk, size_t ld) {
+__device__ __forceinline__ void win_init(ColWin& w, SweepRing& r, int side, const IfcState* X, const double* P, int nk,
+                                         size_t ld) {
     w.k = 1;
+    w.side = side;
+    const int i1 = min(1, nk), i2 = min(2, nk);
+    w.a = load_ifc<LD>(X);
+    w.b = load_ifc<LD>(X + (size_t)i1 * ld);
+    w.c = load_ifc<LD>(X + (size_t)i2 * ld);
+    w.pa = LD::ld(P);
+    w.pb = LD::ld(P + (size_t)i1 * ld);
+    w.pc = LD::ld(P + (size_t)i2 * ld);
+    ring_fetch(r, side, 3, X, P, nk, ld);
+    ring_fetch(r, side, 4, X, P, nk, ld);
+}
+
+// k -> k+1: the anchor km1 moves only when k was >= 2. The interface that
+// enters the window was requested two shifts ago (or at set-up); every group
+// but the newest is complete after wait_group 1, and that group is never the
+// one needed (the column's previous shift, or the empty group that closes the
+// set-up, came after it).
+__device__ __forceinline__ void win_advance(ColWin& w, SweepRing& r, const IfcState* X, const double* P, int nk,
+                                            size_t ld) {
+    if (w.k >= 2) {
+        w.a = w.b;
+        w.b = w.c;
+        w.pa = w.pb;
+        w.pb = w.pc;
+        cp_async_wait<1>();
+        const int q = w.k + 1;  // 0-based index of interface km1_new + 2
+        w.c = r.x[q % kSweepRing][w.side][threadIdx.x];
+        w.pc = r.p[q % kSweepRing][w.side][threadIdx.x];
+        ring_fetch(r, w.side, q + 2, X, P, nk, ld);
+        cp_async_commit();
+    }
+    w.k += 1;
+}
+
+// Register-only variant of the window (the persistent multi-domain kernel):
+// the interface entering the window is loaded straight into it.
+template <class LD>
+__device__ __forceinline__ void win_init_reg(ColWin& w, const IfcState* X, const double* P, int nk, size_t ld) {
+    w.k = 1;
+    w.side = 0;
     const int i1 = min(1, nk), i2 = min(2, nk);
     w.a = load_ifc<LD>(X);
     w.b = load_ifc<LD>(X + (size_t)i1 * ld);
@@ -150,9 +252,8 @@ __device__ __forceinline__ void win_init(ColWin& w, const IfcState* X, const dou
     w.pc = LD::ld(P + (size_t)i2 * ld);
 }
 
-// k -> k+1: the anchor km1 moves only when k was >= 2.
 template <class LD>
-__device__ __forceinline__ void win_advance(ColWin& w, const IfcState* X, const double* P, int nk, size_t ld) {
+__device__ __forceinline__ void win_advance_reg(ColWin& w, const IfcState* X, const double* P, int nk, size_t ld) {
     if (w.k >= 2) {
         w.a = w.b;
         w.b = w.c;
@@ -176,7 +277,9 @@ __device__ __forceinline__ IfcState sel(bool c, const IfcState& x, const IfcStat
 
 __device__ __forceinline__ IfcState win_own(const ColWin& w) { return sel(w.k == 1, w.a, w.b); }
 
-template <class P, class LD>
+// STAGED: the window's look-ahead goes through the shared-memory ring (the
+// standalone sweep kernel); otherwise registers only (the persistent kernel).
+template <class P, class LD, bool STAGED>
 __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int t) {
     const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
     const size_t ld = (size_t)nx * ny;  // interface stride of the scratch
@@ -228,9 +331,17 @@ __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int 
     const double pa_to_h = 1.0 / (kGravity * a.rho0);
     const int nk = nz;
 
+    __shared__ SweepRing ring;
     ColWin wl, wr;
-    win_init<LD>(wl, XL, PL, nk, ld);
-    win_init<LD>(wr, XR, PR, nk, ld);
+    if constexpr (STAGED) {
+        win_init<LD>(wl, ring, 0, XL, PL, nk, ld);
+        win_init<LD>(wr, ring, 1, XR, PR, nk, ld);
+        cp_async_commit();  // the set-up group
+        cp_async_commit();  // an empty group: the set-up group is never the newest
+    } else {
+        win_init_reg<LD>(wl, XL, PL, nk, ld);
+        win_init_reg<LD>(wr, XR, PR, nk, ld);
+    }
     double lastP_left = 0.0, lastP_right = 0.0;
     int lastK_left = 1, lastK_right = 1;
     bool reached_bottom = false, search_left = false, search_right = false;
@@ -261,7 +372,7 @@ __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int 
         const double Spa = L ? wl.pa : wr.pa, Spb = L ? wl.pb : wr.pb, Spc = L ? wl.pc : wr.pc;
         const int Sk = L ? kl : kr;
         const IfcState anc = L ? (kr == 1 ? wr.a : wr.b) : (kl == 1 ? wl.a : wl.b);
-        const double Apa = L ? wr.pa : wl.pa, Apb = L ? wr.pb : wl.pb, Apc = L ? wr.pc : wl.pc;
+        const double Apa = L ? wr.pa : wl.pa, Apb = L ? wr.pb : wl.pb;
         const int ka = L ? kr : kl;
         const double dRhoTop = secant_drho(Sa, anc);
         const double dRhoBot = secant_drho(Sb, anc);
@@ -295,17 +406,25 @@ __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int 
         double po_a, abs_a;
         int ko_a;
         if (ka <= nk) {
+            // redi_absolute_position at po = 0: P(k) + 0*(P(k+1) - P(k)) is
+            // P(k) itself for finite pressures, so the next interface's
+            // pressure (often fetched by the previous step) is not waited on.
             po_a = 0.0;
             ko_a = ka;
-            abs_a = (ka == 1) ? Apa + po_a * (Apb - Apa) : Apb + po_a * (Apc - Apb);
+            abs_a = (ka == 1) ? Apa : Apb;
         } else {
             po_a = 1.0;
             ko_a = nk;
             abs_a = Apa + po_a * (Apb - Apa);  // km1 = nk: interfaces nk, nk+1
         }
         if (ka <= nk) {
-            if (L) win_advance<LD>(wr, XR, PR, nk, ld);
-            else   win_advance<LD>(wl, XL, PL, nk, ld);
+            if constexpr (STAGED) {
+                if (L) win_advance(wr, ring, XR, PR, nk, ld);
+                else   win_advance(wl, ring, XL, PL, nk, ld);
+            } else {
+                if (L) win_advance_reg<LD>(wr, XR, PR, nk, ld);
+                else   win_advance_reg<LD>(wl, XL, PL, nk, ld);
+            }
         } else {
             reached_bottom = true;
             search_left = !L;
@@ -333,6 +452,7 @@ __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int 
         absL_prev = absL;
         absR_prev = absR;
     }
+    if constexpr (STAGED) cp_async_wait<0>();  // no copy may land in the ring after this face is done
 }
 
 // ---------------------------------------------------------------------------
@@ -377,15 +497,13 @@ __device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid) {
     }
     double e_prev[NT];
 
-    auto load = [&](int t, double& hv, double (&sv)[NT]) {
+    auto fetch = [&](int t, RawLayer<NT>& r) {
         const size_t off = (size_t)(nz - t) * ncol;
-        const double hk = LD::ld(h + off);
-        const double he = fmax(hk, kHDivEps);
-        hv = hk;
+        r.h = LD::ld(h + off);
 #pragma unroll
-        for (int n = 0; n < NT; ++n) sv[n] = LD::ld(htr[n] + off) / he;
+        for (int n = 0; n < NT; ++n) r.s[n] = LD::ld(htr[n] + off);
     };
-    auto emit = [&](int t, const double (&e)[NT], const double (&s_above)[NT]) {
+    auto emit = [&](int t, const double (&e)[NT], const double (&s_above)[NT], double) {
 #pragma unroll
         for (int n = 0; n < NT; ++n) {
             if (n < nt) {
@@ -400,7 +518,7 @@ __device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid) {
             e_prev[n] = e[n];
         }
     };
-    stream_edges<NT>(nz, load, emit);
+    stream_edges<NT>(nz, fetch, emit);
 }
 
 // ---------------------------------------------------------------------------

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a) {
 
 template <class P>
 __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgsT<P> a) {
-    sweep_item<P, LdNC>(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+    sweep_item<P, LdNC, true>(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 template <int NT, class P>
