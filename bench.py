@@ -438,7 +438,7 @@ def run_domains(args, rank, world, local_rank):
     from more_benchmarks_dc_ocean_b200 import ocean_redi as R
 
     # Inputs are generated before the first GPU call (the pool is spawned).
-    workers = max(1, min(len(os.sched_getaffinity(0)), 16))
+    workers = max(1, min(len(os.sched_getaffinity(0)), 8))  # host memory: one large domain per worker
     t_gen = time.perf_counter()
     ps = inputs.config4(seed=20261203 + 1000 * rank, n_domains=args.domains, workers=workers)
     t_gen = time.perf_counter() - t_gen
