@@ -75,8 +75,15 @@ typedef struct redi_b200_metrics {
     const double* wet_v; /* (nx, ny+1) */
 } redi_b200_metrics;
 
-/* ocean_eos_t, LINEAR variant (redi/ocean_eos.F90:239-278). variant must be 0
- * (EOS_VARIANT_LINEAR), the only variant any Redi configuration reaches. */
+/* ocean_eos_t (redi/ocean_eos.F90:239-278). variant takes the reference's
+ * codes (ocean_eos.F90:39-51): REDI_B200_EOS_LINEAR (0 is accepted as LINEAR,
+ * a zero-initialised struct), REDI_B200_EOS_WRIGHT_97, REDI_B200_EOS_ROQUET_SPV;
+ * 3 (TEOS-10) is reserved in the reference and rejected with E_UNSUPPORTED.
+ * The linear coefficients are read by the LINEAR branch only; rho0 also sets
+ * the hydrostatic interface pressure for every variant (ocean_redi.F90:643-646). */
+#define REDI_B200_EOS_LINEAR 1
+#define REDI_B200_EOS_WRIGHT_97 2
+#define REDI_B200_EOS_ROQUET_SPV 4
 typedef struct redi_b200_eos {
     int variant;
     double rho0, T_ref, S_ref, alpha_T, beta_S;
@@ -172,6 +179,13 @@ REDI_B200_API int redi_b200_kernel_count(void);
  * (4, 8 or 16). Results do not depend on it; the autotuner picks it. */
 REDI_B200_API int redi_b200_set_tuning(int bx, int by, int chunk);
 REDI_B200_API int redi_b200_get_tuning(int* bx, int* by, int* chunk);
+
+/* eos_density_point and eos_specvol_derivs (redi/ocean_eos.F90:450-546), the
+ * reference's public point routines, at n points: T, S, p (Pa) and the outputs
+ * rho, dSV/dT, dSV/dS are device arrays of n doubles. The values are exactly
+ * those the column state uses at each interface. Stream-ordered. */
+REDI_B200_API int redi_b200_eos_points(const redi_b200_eos* eos, int n, const double* T, const double* S,
+                                       const double* p, double* rho, double* dsv_dt, double* dsv_ds, void* stream);
 
 /* Largest number of tracers whose face fluxes one launch computes (1, 2, 4
  * or 8; default 8), process-wide (no counterpart in the reference). Larger

@@ -112,7 +112,7 @@ bool dims_ok(int nx, int ny, int nz, std::string& why) {
 
 // Phase A into caller-provided or handle-owned coefficient slots.
 template <class P>
-int run_phase_a(int nx, int ny, int nz, const redi::EosLin& eos, const double* h, const double* th,
+int run_phase_a(int nx, int ny, int nz, const redi::EosParams& eos, const double* h, const double* th,
                 const double* sh, const double* wet_u, const double* wet_v, const redi::FaceOutT<P>& u,
                 const redi::FaceOutT<P>& v, Scratch& ws, cudaStream_t st) {
     cudaError_t e = ws.reserve(redi::phase_a_scratch(nx, ny, nz));
@@ -311,6 +311,20 @@ int redi_b200_set_tracer_group(int max_group) {
 
 int redi_b200_get_tracer_group(void) { return redi::cell_tuning().group; }
 
+int redi_b200_eos_points(const redi_b200_eos* eos, int n, const double* T, const double* S, const double* p,
+                         double* rho, double* dsv_dt, double* dsv_ds, void* stream) {
+    if (!eos || n < 0) return fail(REDI_B200_E_ARG, "redi_b200_eos_points: NULL eos or negative count");
+    if (eos->variant == 3)
+        return fail(REDI_B200_E_UNSUPPORTED, "redi_b200_eos_points: EOS variant 3 (TEOS-10) is reserved, not implemented");
+    if (eos->variant != 0 && eos->variant != 1 && eos->variant != 2 && eos->variant != 4)
+        return fail(REDI_B200_E_ARG, "redi_b200_eos_points: unknown EOS variant (1 LINEAR, 2 WRIGHT_97, 4 ROQUET_SPV)");
+    if (n == 0) return REDI_B200_OK;
+    if (!T || !S || !p || !rho || !dsv_dt || !dsv_ds) return fail(REDI_B200_E_ARG, "redi_b200_eos_points: NULL array");
+    const redi::EosParams e{eos->variant, eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
+    cudaError_t err = redi::launch_eos_points(e, n, T, S, p, rho, dsv_dt, dsv_ds, reinterpret_cast<cudaStream_t>(stream));
+    return err == cudaSuccess ? REDI_B200_OK : cuda_fail(err, "redi_b200_eos_points launch");
+}
+
 int redi_b200_get_tuning(int* bx, int* by, int* chunk) {
     if (!bx || !by || !chunk) return fail(REDI_B200_E_ARG, "redi_b200_get_tuning: NULL argument");
     const redi::CellTuning t = redi::cell_tuning();
@@ -473,7 +487,10 @@ int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* m
     if (s->nz_ml != nz) return REDI_B200_SKIPPED;
     if (nx != s->nx_total || ny != s->ny_total)
         return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: grid extents differ from the handle's");
-    if (eos->variant != 0) return fail(REDI_B200_E_UNSUPPORTED, "redi_b200_calc_coeffs: only the LINEAR EOS is supported");
+    if (eos->variant == 3)
+        return fail(REDI_B200_E_UNSUPPORTED, "redi_b200_calc_coeffs: EOS variant 3 (TEOS-10) is reserved, not implemented");
+    if (eos->variant != 0 && eos->variant != 1 && eos->variant != 2 && eos->variant != 4)
+        return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: unknown EOS variant (1 LINEAR, 2 WRIGHT_97, 4 ROQUET_SPV)");
     if (ms->idx_temperature > ms->ntracers || ms->idx_salinity > ms->ntracers || !ms->hTr)
         return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: temperature/salinity index outside the tracer table");
     const double* th = ms->hTr[ms->idx_temperature - 1];
@@ -482,7 +499,7 @@ int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* m
         return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: NULL device array");
     if (!aligned(ms->h_layer) || !aligned(th) || !aligned(sh) || !aligned(metrics->wet_u) || !aligned(metrics->wet_v))
         return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: misaligned device array");
-    redi::EosLin e{eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
+    redi::EosParams e{eos->variant, eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (s->precision == REDI_B200_MIXED)
         return run_phase_a<redi::MixedPrec>(nx, ny, nz, e, ms->h_layer, th, sh, metrics->wet_u, metrics->wet_v,
@@ -592,7 +609,7 @@ static void compat_launch(const char* name, const int* nx_, const int* ny_, cons
     if ((int)g_compat_ws.size() <= dev) g_compat_ws.resize(dev + 1);
     Scratch& ws = g_compat_ws[dev];
     cudaStream_t st = 0;  // the reference launches on the legacy default stream
-    redi::EosLin e{*rho0_, *T_ref_, *S_ref_, *alpha_T_, *beta_S_};
+    redi::EosParams e{1, *rho0_, *T_ref_, *S_ref_, *alpha_T_, *beta_S_};  // the launcher's LINEAR EOS
     redi::FaceOut u{uPoL, uPoR, uKoL, uKoR, uhEff}, v{vPoL, vPoR, vKoL, vKoR, vhEff};
     int rc = run_phase_a<redi::PlainPrec>(nx, ny, nz, e, h_layer, t_htr, s_htr, wet_u, wet_v, u, v, ws, st);
     if (rc < 0) { report(rc, g_last_error); return; }

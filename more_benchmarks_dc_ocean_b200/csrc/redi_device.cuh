@@ -35,9 +35,15 @@ constexpr double kGravity = 9.80665;    // redi/constants.F90:19
 constexpr double kHDivEps = 1.0e-20;    // redi/constants.F90:21
 constexpr double kHNeglect = 1.0e-30;   // ocean_redi.F90:242
 
-struct EosLin {  // ocean_eos.F90:239-278, the members the LINEAR branch reads
+// ocean_eos_t (ocean_eos.F90:239-278): the variant (the reference's codes,
+// :39-51: 1 LINEAR, 2 WRIGHT_97, 4 ROQUET_SPV; 0 is LINEAR) and the members the
+// LINEAR branch reads. rho0 also sets the hydrostatic pressure in every
+// variant (ocean_redi.F90:643-646).
+struct EosParams {
+    int variant;
     double rho0, T_ref, S_ref, alpha_T, beta_S;
 };
+__host__ __device__ inline bool eos_is_linear(int variant) { return variant == 0 || variant == 1; }
 
 // -------------------------------------------------------------------------
 // PLM slope geometry at top-down layer t (ocean_redi.F90:135-150, 174-176):

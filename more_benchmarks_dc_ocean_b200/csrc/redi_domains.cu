@@ -345,8 +345,10 @@ int build(redi_b200_batch* b, int n, const redi_b200_domain* dom) {
                                               " needs 2..64 tracers and a thickness field");
         if (D.ms.idx_temperature < 1 || D.ms.idx_salinity < 1 || D.ms.idx_temperature > ntr || D.ms.idx_salinity > ntr)
             return bfail(REDI_B200_E_ARG, "redi_b200_batch_create: domain " + std::to_string(k) + " has no T/S");
-        if (D.eos.variant != 0)
-            return bfail(REDI_B200_E_UNSUPPORTED, "redi_b200_batch_create: only the LINEAR EOS is supported");
+        if (D.eos.variant != 0 && D.eos.variant != 1 && D.eos.variant != 2 && D.eos.variant != 4)
+            return bfail(D.eos.variant == 3 ? REDI_B200_E_UNSUPPORTED : REDI_B200_E_ARG,
+                         "redi_b200_batch_create: domain " + std::to_string(k) +
+                             ": EOS variant must be 1 LINEAR, 2 WRIGHT_97 or 4 ROQUET_SPV");
         if (!D.khtr_u_ext || !D.khtr_v_ext || !D.metrics.dy_cu || !D.metrics.dx_cv || !D.metrics.idxCu ||
             !D.metrics.idyCv || !D.metrics.areaT || !D.metrics.wet_u || !D.metrics.wet_v)
             return bfail(REDI_B200_E_ARG, "redi_b200_batch_create: domain " + std::to_string(k) + " has a NULL array");
@@ -376,8 +378,8 @@ int build(redi_b200_batch* b, int n, const redi_b200_domain* dom) {
         std::memset(&d, 0, sizeof(d));
         const double* th = D.ms.hTr[D.ms.idx_temperature - 1];
         const double* sh = D.ms.hTr[D.ms.idx_salinity - 1];
-        d.cs = redi::ColumnStateArgs{nx, ny, nz, redi::EosLin{D.eos.rho0, D.eos.T_ref, D.eos.S_ref, D.eos.alpha_T,
-                                                               D.eos.beta_S},
+        d.cs = redi::ColumnStateArgs{nx, ny, nz, redi::EosParams{D.eos.variant, D.eos.rho0, D.eos.T_ref, D.eos.S_ref,
+                                                                  D.eos.alpha_T, D.eos.beta_S},
                                      D.ms.h_layer, th, sh, (redi::IfcState*)sc, nullptr};
         d.cs.pint = (double*)(d.cs.ifc + ncol * (nz + 1));
         d.sw.nx = nx; d.sw.ny = ny; d.sw.nz = nz; d.sw.rho0 = D.eos.rho0;

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "redi_device.cuh"
+#include "redi_eos.cuh"
 #include "redi_kernels.h"
 
 namespace redi {
@@ -115,7 +116,8 @@ __device__ __forceinline__ void column_state_item(const ColumnStateArgs& a, int 
     IfcState* __restrict__ ifc = a.ifc + col;
     double* __restrict__ pint = a.pint + col;
 
-    const EosLin eos = a.eos;
+    const EosParams eos = a.eos;
+    const bool linear = eos_is_linear(eos.variant);  // uniform over the launch
     const double dsv_dt = eos.alpha_T / (eos.rho0 * eos.rho0);  // ocean_eos.F90:511
     const double dsv_ds = -eos.beta_S / (eos.rho0 * eos.rho0);  // ocean_eos.F90:512
     const double grho = kGravity * eos.rho0;
@@ -130,10 +132,14 @@ __device__ __forceinline__ void column_state_item(const ColumnStateArgs& a, int 
     };
     auto emit = [&](int t, const double (&e)[2], const double (&)[2], double h_t) {
         if (t >= 2) P = P + grho * h_layer_above;  // Pint(t) = Pint(t-1) + g*rho0*h(t-1)
-        const double rho_i = eos.rho0 + eos.beta_S * (e[1] - eos.S_ref) - eos.alpha_T * (e[0] - eos.T_ref);
+        double rho_i, sv_t = dsv_dt, sv_s = dsv_ds;
+        if (linear)
+            rho_i = eos.rho0 + eos.beta_S * (e[1] - eos.S_ref) - eos.alpha_T * (e[0] - eos.T_ref);
+        else  // WRIGHT_97 / ROQUET_SPV at the interface pressure (ocean_redi.F90:649-650)
+            eos::nonlinear_point(eos.variant, e[0], e[1], P, rho_i, sv_t, sv_s);
         double2* q = reinterpret_cast<double2*>(ifc + (size_t)(t - 1) * ncol);
         q[0] = make_double2(e[0], e[1]);
-        q[1] = make_double2(-(rho_i * rho_i) * dsv_dt, -(rho_i * rho_i) * dsv_ds);
+        q[1] = make_double2(-(rho_i * rho_i) * sv_t, -(rho_i * rho_i) * sv_s);
         pint[(size_t)(t - 1) * ncol] = P;
         h_layer_above = h_t;
     };

@@ -69,7 +69,7 @@ using FaceIn = FaceInT<PlainPrec>;
 
 struct ColumnStateArgs {
     int nx, ny, nz;
-    EosLin eos;
+    EosParams eos;
     const double* h;
     const double* th;
     const double* sh;
@@ -195,6 +195,9 @@ CellTuning cell_tuning();
 void set_cell_tuning(const CellTuning& t);
 
 cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st);
+// Density and dSV/dT, dSV/dS at n points (T, S, p device arrays).
+cudaError_t launch_eos_points(const EosParams& e, int n, const double* T, const double* S, const double* p,
+                              double* rho, double* dsv_dt, double* dsv_ds, cudaStream_t st);
 template <class P>
 cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st);
 template <class P>

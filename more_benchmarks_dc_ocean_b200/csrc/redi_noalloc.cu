@@ -124,7 +124,7 @@ int redi_b200_opt_launch_noalloc(const int* nx_, const int* ny_, const int* nz_,
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
 
     // Phase A (redi_calc_coeffs).
-    redi::EosLin eos{*rho0_, *T_ref_, *S_ref_, *alpha_T_, *beta_S_};
+    redi::EosParams eos{1, *rho0_, *T_ref_, *S_ref_, *alpha_T_, *beta_S_};  // the launcher's LINEAR EOS
     redi::ColumnStateArgs cs{};
     cs.nx = nx; cs.ny = ny; cs.nz = nz; cs.eos = eos; cs.h = h_layer; cs.th = t_htr; cs.sh = s_htr;
     cs.ifc = reinterpret_cast<redi::IfcState*>(data);

@@ -70,6 +70,24 @@ __global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgsT<P> a, int t
                                  tr0, fslot);
 }
 
+// The point EOS at n independent points, as the column state evaluates it at
+// each interface (eos_density_point + eos_specvol_derivs).
+__global__ void __launch_bounds__(128) k_eos_points(EosParams e, int n, const double* __restrict__ T,
+                                                    const double* __restrict__ S, const double* __restrict__ p,
+                                                    double* __restrict__ rho, double* __restrict__ dsv_dt,
+                                                    double* __restrict__ dsv_ds) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double r, a = e.alpha_T / (e.rho0 * e.rho0), b = -e.beta_S / (e.rho0 * e.rho0);
+    if (eos_is_linear(e.variant))
+        r = e.rho0 + e.beta_S * (S[i] - e.S_ref) - e.alpha_T * (T[i] - e.T_ref);
+    else
+        eos::nonlinear_point(e.variant, T[i], S[i], p[i], r, a, b);
+    rho[i] = r;
+    dsv_dt[i] = a;
+    dsv_ds[i] = b;
+}
+
 }  // namespace plain
 
 // ---------------------------------------------------------------------------
@@ -80,6 +98,15 @@ cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st) {
     launch_begin(K_COLUMN_STATE, st);
     plain::k_column_state<<<(ncol + 127) / 128, 128, 0, st>>>(cs);
     launch_end(K_COLUMN_STATE, st);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eos_points(const EosParams& e, int n, const double* T, const double* S, const double* p,
+                              double* rho, double* dsv_dt, double* dsv_ds, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    launch_begin(K_AUX, st);
+    plain::k_eos_points<<<(n + 127) / 128, 128, 0, st>>>(e, n, T, S, p, rho, dsv_dt, dsv_ds);
+    launch_end(K_AUX, st);
     return cudaGetLastError();
 }
 

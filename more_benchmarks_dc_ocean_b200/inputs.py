@@ -55,13 +55,15 @@ _F_SEAMOUNTS, _F_LAYERS, _F_TNOISE, _F_SNOISE, _F_PASSIVE0 = 1, 2, 3, 4, 100
 
 @dataclass
 class Eos:
-    """Linear equation of state (redi/ocean_eos.F90:239-278, LINEAR branch)."""
+    """ocean_eos_t (redi/ocean_eos.F90:239-278): the variant (1 LINEAR, 2 WRIGHT_97,
+    4 ROQUET_SPV, the reference's codes) and the linear branch's coefficients."""
 
     rho0: float = 1035.0
     T_ref: float = 10.0
     S_ref: float = 35.0
     alpha_T: float = 1.7e-4
     beta_S: float = 7.6e-4
+    variant: int = 1
 
 
 @dataclass

@@ -172,16 +172,20 @@ class OceanMetrics:
                                                             "wet_v")))
 
 
+EOS_LINEAR, EOS_WRIGHT_97, EOS_ROQUET_SPV = 1, 2, 4  # redi/ocean_eos.F90:39-51
+
+
 @dataclass
 class OceanEos:
-    """ocean_eos_t, LINEAR variant (redi/ocean_eos.F90:239-278)."""
+    """ocean_eos_t (redi/ocean_eos.F90:239-278): variant (EOS_LINEAR, EOS_WRIGHT_97,
+    EOS_ROQUET_SPV; 0 is taken as LINEAR) and the linear branch's coefficients."""
 
     rho0: float = 1035.0
     T_ref: float = 10.0
     S_ref: float = 35.0
     alpha_T: float = 1.7e-4
     beta_S: float = 7.6e-4
-    variant: int = 0
+    variant: int = EOS_LINEAR
 
     def _c(self) -> _Eos:
         return _Eos(self.variant, self.rho0, self.T_ref, self.S_ref, self.alpha_T, self.beta_S)
@@ -398,10 +402,26 @@ def to_device(p, device="cuda", tracers: Optional[Sequence[np.ndarray]] = None) 
     return DeviceProblem(
         grid=HGrid(p.nx, p.ny, p.nx_phys, p.ny_phys, p.nghost, 0.0, 0.0),
         metrics=OceanMetrics(d(p.dy_cu), d(p.dx_cv), d(p.idxCu), d(p.idyCv), d(p.areaT), d(p.wet_u), d(p.wet_v)),
-        eos=OceanEos(p.eos.rho0, p.eos.T_ref, p.eos.S_ref, p.eos.alpha_T, p.eos.beta_S),
+        eos=OceanEos(p.eos.rho0, p.eos.T_ref, p.eos.S_ref, p.eos.alpha_T, p.eos.beta_S,
+                     getattr(p.eos, "variant", EOS_LINEAR)),
         ms=MultilayerState(p.nz, d(p.h), trs, p.idx_temperature + 1, p.idx_salinity + 1),
         khtr_u_ext=d(p.khtr_u), khtr_v_ext=d(p.khtr_v),
         bc=OceanBC(wall(ww), wall(we), wall(ws), wall(wn)), dt=p.dt)
+
+
+def eos_points(eos: OceanEos, T, S, p, stream=None):
+    """eos_density_point + eos_specvol_derivs (redi/ocean_eos.F90:450-546) at every point of the
+    float64 CUDA tensors T, S, p (Pa); returns (rho, dsv_dt, dsv_ds) tensors."""
+    import torch
+
+    L = lib()
+    L.redi_b200_eos_points.argtypes = [C.POINTER(_Eos), C.c_int] + [C.c_void_p] * 7
+    T, S, p = (t.contiguous() for t in (T, S, p))
+    out = [torch.empty_like(T) for _ in range(3)]
+    e = eos._c()
+    _check(L.redi_b200_eos_points(C.byref(e), T.numel(), _ptr(T), _ptr(S), _ptr(p), *[_ptr(o) for o in out],
+                                  _stream(stream)))
+    return tuple(out)
 
 
 def make_redi(dp: DeviceProblem, precision: int = FP64) -> OceanRedi:

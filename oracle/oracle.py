@@ -36,12 +36,15 @@ def lib():
     global _lib
     with _lock:
         if _lib is None:
-            if not os.path.exists(_LIB_PATH) or (
-                os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "redi_oracle.cpp"))
-            ):
+            srcs = [os.path.join(_HERE, f) for f in ("redi_oracle.cpp", "redi_eos_oracle.h")]
+            if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < max(map(os.path.getmtime, srcs)):
                 build()
             L = C.CDLL(_LIB_PATH)
             L.redi_oracle_calc_coeffs.restype = None
+            L.redi_oracle_eos_point.restype = None
+            L.redi_oracle_eos_point.argtypes = [C.c_int] + [C.c_double] * 8 + [_dp] * 3
+            L.redi_oracle_roquet_sv.restype = C.c_double
+            L.redi_oracle_roquet_sv.argtypes = [C.c_double] * 3
             L.redi_oracle_apply_flux.restype = None
             L.redi_oracle_count_ops.restype = None
             L.redi_oracle_max_threads.restype = C.c_int
@@ -82,8 +85,23 @@ def calc_coeffs(p, coeffs: dict | None = None, nthreads: int = 0) -> dict:
         p.nx, p.ny, p.nz, p.ns, C.c_double(e.rho0), C.c_double(e.T_ref), C.c_double(e.S_ref),
         C.c_double(e.alpha_T), C.c_double(e.beta_S), _d(p.h), _d(T), _d(S), _d(p.wet_u), _d(p.wet_v),
         _d(c["uPoL"]), _d(c["uPoR"]), _i(c["uKoL"]), _i(c["uKoR"]), _d(c["uhEff"]),
-        _d(c["vPoL"]), _d(c["vPoR"]), _i(c["vKoL"]), _i(c["vKoR"]), _d(c["vhEff"]), nthreads)
+        _d(c["vPoL"]), _d(c["vPoR"]), _i(c["vKoL"]), _i(c["vKoR"]), _d(c["vhEff"]), nthreads,
+        int(getattr(e, "variant", 1)))
     return c
+
+
+def eos_point(eos, T: float, S: float, p: float):
+    """(rho, dSV/dT, dSV/dS) at one point, as redi_build_column combines the reference's
+    eos_density_point and eos_specvol_derivs (ocean_eos.F90:450-546)."""
+    out = [C.c_double() for _ in range(3)]
+    lib().redi_oracle_eos_point(int(getattr(eos, "variant", 1)), eos.rho0, eos.T_ref, eos.S_ref, eos.alpha_T,
+                                eos.beta_S, float(T), float(S), float(p), *[C.byref(o) for o in out])
+    return tuple(o.value for o in out)
+
+
+def roquet_sv(T: float, S: float, p: float) -> float:
+    """Specific volume of the Roquet (2015) polynomial (roquet_spv_point's sv)."""
+    return lib().redi_oracle_roquet_sv(float(T), float(S), float(p))
 
 
 def apply_flux(p, coeffs: dict, tracers=None, nthreads: int = 0):

@@ -6,7 +6,8 @@
 //
 // It restates, function by function, the reference's do-concurrent Fortran
 // (redi/ocean_redi.F90, the "faithful" path that `make verify` / `DATA=none`
-// runs on the CPU) and the LINEAR branch of redi/ocean_eos.F90. Every
+// runs on the CPU) and the point EOS of redi/ocean_eos.F90 (LINEAR here, the
+// WRIGHT_97 and ROQUET_SPV branches in redi_eos_oracle.h). Every
 // floating-point expression keeps the reference's operand order and
 // association (Fortran evaluates a*b*c as (a*b)*c, as the reference's own CUDA
 // transliteration redi/redi_kernel.cu does). Build with
@@ -32,8 +33,11 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 #include <omp.h>
+
+#include "redi_eos_oracle.h"
 
 namespace {
 
@@ -81,8 +85,9 @@ template <> inline double r_from_int<double>(int k) { return static_cast<double>
 template <> inline OpCount r_from_int<OpCount>(int k) { g_tally.cvt++; return OpCount(static_cast<double>(k)); }
 
 template <class R>
-struct Eos {  // ocean_eos.F90:239-278 (the scalar members the LINEAR branch reads)
+struct Eos {  // ocean_eos.F90:239-278 (the scalar members the point routines read)
     R rho0, T_ref, S_ref, alpha_T, beta_S;
+    int variant;  // ocean_eos.F90:39-51: 1 (or 0) LINEAR, 2 WRIGHT_97, 4 ROQUET_SPV
 };
 
 // ---- ocean_eos.F90:543-545 eos_density_point, LINEAR -----------------------
@@ -317,8 +322,18 @@ void build_column(int nz, const R* h_col, const R* thtr_col, const R* shtr_col, 
     for (int k = 1; k <= nz; ++k) Pint[k] = Pint[k - 1] + R(GRAVITY) * eos.rho0 * w.htd[k - 1];
     R dsv_dt, dsv_ds;
     for (int k = 1; k <= nz + 1; ++k) {
-        R rho_i = eos_density_point(eos, Tint[k - 1], Sint[k - 1]);
-        eos_specvol_derivs(eos, dsv_dt, dsv_ds);
+        R rho_i;
+        if constexpr (std::is_same<R, double>::value) {
+            if (eos.variant == 2 || eos.variant == 4) {  // WRIGHT_97 / ROQUET_SPV at the interface pressure
+                eos_oracle::point(eos.variant, Tint[k - 1], Sint[k - 1], Pint[k - 1], rho_i, dsv_dt, dsv_ds);
+            } else {
+                rho_i = eos_density_point(eos, Tint[k - 1], Sint[k - 1]);
+                eos_specvol_derivs(eos, dsv_dt, dsv_ds);
+            }
+        } else {  // operation counts: the LINEAR branch
+            rho_i = eos_density_point(eos, Tint[k - 1], Sint[k - 1]);
+            eos_specvol_derivs(eos, dsv_dt, dsv_ds);
+        }
         dRdT[k - 1] = -(rho_i * rho_i) * dsv_dt;
         dRdS[k - 1] = -(rho_i * rho_i) * dsv_ds;
     }
@@ -569,8 +584,8 @@ void redi_oracle_calc_coeffs(int nx, int ny, int nz, int ns, double rho0, double
                              double alpha_T, double beta_S, const double* h, const double* th, const double* sh,
                              const double* wet_u, const double* wet_v, double* uPoL, double* uPoR, int* uKoL,
                              int* uKoR, double* uhEff, double* vPoL, double* vPoR, int* vKoL, int* vKoR,
-                             double* vhEff, int nthreads) {
-    Eos<double> e{rho0, T_ref, S_ref, alpha_T, beta_S};
+                             double* vhEff, int nthreads, int eos_variant) {
+    Eos<double> e{rho0, T_ref, S_ref, alpha_T, beta_S, eos_variant};
     nthreads = resolve_threads(nthreads);
     calc_coeffs_dir<double>(0, nx, ny, nz, ns, e, h, th, sh, wet_u, uPoL, uPoR, uKoL, uKoR, uhEff, nthreads);
     calc_coeffs_dir<double>(1, nx, ny, nz, ns, e, h, th, sh, wet_v, vPoL, vPoR, vKoL, vKoR, vhEff, nthreads);
@@ -610,7 +625,7 @@ void redi_oracle_count_ops(int nx, int ny, int nz, int ns, double rho0, double T
                            const double* dx_cv, const double* idxCu, const double* idyCv, const double* areaT,
                            double* uPoL, double* uPoR, int* uKoL, int* uKoR, double* uhEff, double* vPoL,
                            double* vPoR, int* vKoL, int* vKoR, double* vhEff, uint64_t* outA, uint64_t* outB) {
-    Eos<OpCount> e{rho0, T_ref, S_ref, alpha_T, beta_S};
+    Eos<OpCount> e{rho0, T_ref, S_ref, alpha_T, beta_S, 1};
     g_tally = OpTally{};
     calc_coeffs_dir<OpCount>(0, nx, ny, nz, ns, e, h, htr[0], htr[1], wet_u, uPoL, uPoR, uKoL, uKoR, uhEff, 1);
     calc_coeffs_dir<OpCount>(1, nx, ny, nz, ns, e, h, htr[0], htr[1], wet_v, vPoL, vPoR, vKoL, vKoR, vhEff, 1);
@@ -629,5 +644,26 @@ void redi_oracle_count_ops(int nx, int ny, int nz, int ns, double rho0, double T
 }
 
 int redi_oracle_max_threads(void) { return omp_get_max_threads(); }
+
+// One interface's density and specific-volume derivatives, as the column
+// builder combines eos_density_point and eos_specvol_derivs
+// (ocean_redi.F90:649-653), for every variant.
+void redi_oracle_eos_point(int variant, double rho0, double T_ref, double S_ref, double alpha_T, double beta_S,
+                           double T, double S, double p, double* rho, double* dsv_dt, double* dsv_ds) {
+    Eos<double> e{rho0, T_ref, S_ref, alpha_T, beta_S, variant};
+    if (variant == 2 || variant == 4) {
+        eos_oracle::point(variant, T, S, p, *rho, *dsv_dt, *dsv_ds);
+    } else {
+        *rho = eos_density_point(e, T, S);
+        eos_specvol_derivs(e, *dsv_dt, *dsv_ds);
+    }
+}
+
+// Specific volume of the Roquet polynomial alone (roquet_spv_point's `sv`).
+double redi_oracle_roquet_sv(double T, double S, double p) {
+    double sv, a, b;
+    eos_oracle::roquet_point(T, S, p, sv, a, b);
+    return sv;
+}
 
 }  // extern "C"

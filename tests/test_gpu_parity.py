@@ -195,7 +195,7 @@ def test_invalid_arguments_raise(redi_lib):
     bad = R.HGrid(p.nx + 1, p.ny, p.nx_phys, p.ny_phys, p.nghost)
     with pytest.raises(R.RediError):
         R.redi_calc_coeffs(bad, dp.metrics, dp.eos, redi, dp.ms)
-    eos = R.OceanEos(variant=1)
+    eos = R.OceanEos(variant=3)  # EOS_VARIANT_TEOS10: reserved in the reference (ocean_eos.F90:49)
     with pytest.raises(R.RediError):
         R.redi_calc_coeffs(dp.grid, dp.metrics, eos, redi, dp.ms)
     redi.destroy()
