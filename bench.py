@@ -13,7 +13,9 @@ Metric: tracer-cell updates/s = N_tracers * nx_phys * ny_phys * 
   no flush is needed between steps.
 * e2e: the same metric through the public entry points with the model state
   resident in pinned HOST memory: every step copies h and every tracer host to
-  device, runs the step and copies every tracer back.
+  device, runs the step and copies every tracer back. On one GPU this is
+  redi_b200_step_host, which pipelines the copies and the kernels over row
+  bands; with halo exchange (N > 1) the copies wrap the device entry points.
 * roofline: the dominant kernel (most device time in the timed region, from
   CUDA event pairs the library records around each launch on its stream);
   achieved = algorithmic bytes per launch / mean launch time.
@@ -680,17 +682,40 @@ def _e2e(args, p, dp, redi, ex, st, dist, dev, world):
 
     host_h = torch.from_numpy(np.ascontiguousarray(p.h)).pin_memory()
     host_tr = [torch.from_numpy(np.ascontiguousarray(t)).pin_memory() for t in p.tracers]
+    path, bands, band_ms = "copies around the device entry points", None, None
 
-    def e2e_step():
-        dp.ms.h_layer.copy_(host_h, non_blocking=True)
-        for d, h in zip(dp.ms.tracers, host_tr):
-            d.copy_(h, non_blocking=True)
-        if ex is not None:
+    if ex is None:
+        # One GPU: the host-state entry point, row bands pipelined through
+        # upload / step / download streams.
+        ms_host = R.MultilayerState(p.nz, host_h, host_tr, p.idx_temperature + 1, p.idx_salinity + 1)
+        bands = 8
+
+        def e2e_step():
+            R.redi_step_host(dp.grid, dp.metrics, dp.eos, redi, ms_host, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext,
+                             dp.bc, bands, st)
+
+        band_ms = {}
+        for nb in (4, 8, 16, 32):  # pick the band count on the live problem (part of the warm-up)
+            bands = nb
+            e2e_step()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            e2e_step()
+            b.record(st)
+            torch.cuda.synchronize()
+            band_ms[nb] = round(a.elapsed_time(b), 2)
+        bands = min(band_ms, key=band_ms.get)
+        path = f"redi_b200_step_host, {bands} row bands"
+    else:
+        def e2e_step():
+            dp.ms.h_layer.copy_(host_h, non_blocking=True)
+            for d, h in zip(dp.ms.tracers, host_tr):
+                d.copy_(h, non_blocking=True)
             ex.exchange()
-        R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, st)
-        R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, st)
-        for d, h in zip(dp.ms.tracers, host_tr):
-            h.copy_(d, non_blocking=True)
+            R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, st)
+            R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, st)
+            for d, h in zip(dp.ms.tracers, host_tr):
+                h.copy_(d, non_blocking=True)
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
@@ -707,7 +732,7 @@ def _e2e(args, p, dp, redi, ex, st, dist, dev, world):
     nt = p.nx * p.ny * p.nz
     return {"value": p.ntr * p.nx_phys * p.ny_phys * p.nz * world / (ms * 1e-3), "unit": UNIT,
             "h2d_bytes_per_step": 8 * nt * (1 + p.ntr), "d2h_bytes_per_step": 8 * nt * p.ntr, "ms_per_step": ms,
-            "host_memory": "pinned"}
+            "host_memory": "pinned", "path": path, "band_candidates_ms": band_ms}
 
 
 def main():

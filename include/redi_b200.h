@@ -145,6 +145,25 @@ REDI_B200_API int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b2
                          const redi_b200_state* ms, double dt, const double* khtr_u_ext, const double* khtr_v_ext,
                          const redi_b200_bc* bc, void* stream);
 
+/* redi_b200_calc_coeffs followed by redi_b200_apply_flux on a model state held
+ * in HOST memory (no counterpart in the reference, whose CPU build keeps its
+ * state on the host and steps it there): ms->h_layer and ms->hTr[t] are host
+ * pointers to the (nx, ny, nz) fields, read and updated in place; metrics and
+ * khtr_u_ext/khtr_v_ext stay device pointers. The step is pipelined over
+ * nbands bands of rows (1..64): rows are copied up on one stream, each band
+ * is stepped as soon as its rows and the next row are on the device, and
+ * finished rows are copied back on a third stream, so host<->device traffic
+ * overlaps the kernels and itself. Results equal the two device entry points
+ * bit for bit. Stream-ordered on `stream`: the host arrays are in use until
+ * the stream reaches this call's end; page-locked host memory is needed for
+ * the copies to overlap. Each phase keeps its own gates; SKIPPED when both
+ * are gated. The handle holds device copies of h and of every tracer (twice)
+ * from the first call on. */
+REDI_B200_API int redi_b200_step_host(const redi_b200_grid* grid, const redi_b200_metrics* metrics,
+                                      const redi_b200_eos* eos, redi_b200* self, const redi_b200_state* ms,
+                                      double dt, const double* khtr_u_ext, const double* khtr_v_ext,
+                                      const redi_b200_bc* bc, int nbands, void* stream);
+
 /* Device pointers of the handle's coefficient slots. */
 REDI_B200_API int redi_b200_get_coeffs(const redi_b200* self, redi_b200_coeffs* out);
 

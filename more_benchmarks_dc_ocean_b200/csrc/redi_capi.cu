@@ -114,7 +114,7 @@ bool dims_ok(int nx, int ny, int nz, std::string& why) {
 template <class P>
 int run_phase_a(int nx, int ny, int nz, const redi::EosParams& eos, const double* h, const double* th,
                 const double* sh, const double* wet_u, const double* wet_v, const redi::FaceOutT<P>& u,
-                const redi::FaceOutT<P>& v, Scratch& ws, cudaStream_t st) {
+                const redi::FaceOutT<P>& v, Scratch& ws, cudaStream_t st, redi::Band band = redi::Band{}) {
     cudaError_t e = ws.reserve(redi::phase_a_scratch(nx, ny, nz));
     if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (phase A)");
     const size_t nifc = (size_t)nx * ny * (nz + 1);
@@ -127,8 +127,8 @@ int run_phase_a(int nx, int ny, int nz, const redi::EosParams& eos, const double
     sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos.rho0;
     sw.wet_u = wet_u; sw.wet_v = wet_v; sw.ifc = cs.ifc; sw.pint = cs.pint;
     sw.u = u; sw.v = v;
-    e = redi::launch_column_state(cs, st);
-    if (e == cudaSuccess) e = redi::launch_sweep<P>(sw, st);
+    e = redi::launch_column_state(cs, st, band);
+    if (e == cudaSuccess) e = redi::launch_sweep<P>(sw, st, band);
     if (e != cudaSuccess) return cuda_fail(e, "phase A launch");
     return REDI_B200_OK;
 }
@@ -142,8 +142,11 @@ struct PhaseBInputs {
     redi::FaceInT<P> u, v;
 };
 
+// htr_in (may be null: in place) holds the pre-step tracers, htr receives the
+// updated ones; band restricts the launches to a band of rows.
 template <class P>
-int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch& ws, cudaStream_t st) {
+int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch& ws, cudaStream_t st,
+                const double* const* htr_in = nullptr, redi::Band band = redi::Band{}) {
     const int batch = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
     const size_t recon = redi::recon_bytes<P>(in.nx, in.ny, in.nz, batch);
     const int group = redi::tracer_group(batch, redi::cell_tuning().group);
@@ -174,13 +177,80 @@ int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch&
         cg.wall_w = in.walls[0]; cg.wall_e = in.walls[1]; cg.wall_s = in.walls[2]; cg.wall_n = in.walls[3];
         cg.areaT = in.areaT; cg.u = in.u; cg.v = in.v; cg.Fu = Fu; cg.Fv = Fv; cg.err = ws.err();
         for (int n = 0; n < nt; ++n) {
-            rc.htr[n] = htr[t0 + n];
+            rc.htr[n] = htr_in ? htr_in[t0 + n] : htr[t0 + n];
             cg.htr[n] = htr[t0 + n];
+            cg.htr_in[n] = htr_in ? htr_in[t0 + n] : htr[t0 + n];
         }
-        e = redi::launch_phase_b<P>(rc, ff, cg, st);
+        e = redi::launch_phase_b<P>(rc, ff, cg, st, band);
         if (e != cudaSuccess) return cuda_fail(e, "phase B launch");
     }
     return REDI_B200_OK;
+}
+
+// Device side of the host-state step: h and the tracers' pre-step and updated
+// copies (the gather reads one and writes the other, so bands can be stepped
+// one after another while their rows stream in and out), and the three
+// streams of the pipeline. Grow-only; released with the handle.
+struct HostPipeline {
+    double* h = nullptr;
+    std::vector<double*> tin, tout;
+    size_t ncell = 0;
+    cudaStream_t up = nullptr, comp = nullptr, down = nullptr;
+    std::vector<cudaEvent_t> ev;
+
+    cudaError_t ensure(size_t n, int ntr, int nevents) {
+        cudaError_t e = cudaSuccess;
+        if (n != ncell || (int)tin.size() < ntr) {
+            release_buffers();
+            ncell = n;
+            e = cudaMalloc((void**)&h, n * 8);
+            tin.assign(ntr, nullptr);
+            tout.assign(ntr, nullptr);
+            for (int t = 0; t < ntr && e == cudaSuccess; ++t) {
+                e = cudaMalloc((void**)&tin[t], n * 8);
+                if (e == cudaSuccess) e = cudaMalloc((void**)&tout[t], n * 8);
+            }
+            if (e != cudaSuccess) {
+                release_buffers();
+                return e;
+            }
+        }
+        if (!up) e = cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
+        if (e == cudaSuccess && !comp) e = cudaStreamCreateWithFlags(&comp, cudaStreamNonBlocking);
+        if (e == cudaSuccess && !down) e = cudaStreamCreateWithFlags(&down, cudaStreamNonBlocking);
+        while (e == cudaSuccess && (int)ev.size() < nevents) {
+            cudaEvent_t x;
+            e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+            if (e == cudaSuccess) ev.push_back(x);
+        }
+        return e;
+    }
+    void release_buffers() {
+        if (h) cudaFree(h);
+        for (double* p : tin) if (p) cudaFree(p);
+        for (double* p : tout) if (p) cudaFree(p);
+        h = nullptr;
+        tin.clear();
+        tout.clear();
+        ncell = 0;
+    }
+    void release() {
+        release_buffers();
+        for (cudaEvent_t x : ev) cudaEventDestroy(x);
+        ev.clear();
+        for (cudaStream_t* s : {&up, &comp, &down})
+            if (*s) cudaStreamDestroy(*s), *s = nullptr;
+    }
+};
+
+// Rows [r0, r1) of an (nx, ny, nz) column-major field: nz slabs of r1-r0
+// consecutive rows, one strided copy.
+cudaError_t copy_rows(double* dst, const double* src, int nx, int ny, int nz, int r0, int r1, cudaMemcpyKind kind,
+                      cudaStream_t st) {
+    if (r1 <= r0) return cudaSuccess;
+    const size_t pitch = (size_t)nx * ny * 8;
+    return cudaMemcpy2DAsync(dst + (size_t)r0 * nx, pitch, src + (size_t)r0 * nx, pitch, (size_t)(r1 - r0) * nx * 8,
+                             nz, kind, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -271,6 +341,7 @@ struct redi_b200 {
         return {o.PoL, o.PoR, o.KoL, o.KoR, o.hEff};
     }
     Scratch ws;
+    HostPipeline host;
     std::vector<void*> allocations;
 
     cudaError_t alloc(void** p, size_t bytes) {
@@ -282,6 +353,7 @@ struct redi_b200 {
         for (void* p : allocations) cudaFree(p);
         allocations.clear();
         ws.release();
+        host.release();
     }
 };
 
@@ -568,6 +640,142 @@ int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* me
     in.u = s->in_u<redi::PlainPrec>();
     in.v = s->in_v<redi::PlainPrec>();
     return run_phase_b<redi::PlainPrec>(in, ms->ntracers, ms->hTr, s->ws, st);
+}
+
+}  // extern "C"
+
+// redi_calc_coeffs followed by redi_apply_flux on a model state that lives in
+// host memory, pipelined over bands of rows: rows stream in on one stream,
+// each band is stepped on a second as soon as its rows (and the row after
+// them) are on the device, and finished rows stream back on a third.
+template <class P>
+int step_host_impl(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi::EosParams& eos,
+                   redi_b200* s, const redi_b200_state* ms, double dt, bool doA, bool doB, int walls[4],
+                   bool use_ext, const double* khtr_u_ext, const double* khtr_v_ext, int nbands, cudaStream_t caller) {
+    const int nx = grid->nx_total, ny = grid->ny_total, nz = ms->nz_ml, ntr = ms->ntracers;
+    const size_t ncell = (size_t)nx * ny * nz;
+    HostPipeline& hp = s->host;
+    cudaError_t e = hp.ensure(ncell, ntr, 2 * nbands + 3);
+    if (e != cudaSuccess) return fail(REDI_B200_E_NOMEM, std::string("redi_b200_step_host: ") + cudaGetErrorString(e));
+    // Scratch for both phases up front: no reallocation while the pipeline runs.
+    const int batch = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
+    const size_t need_b = redi::recon_bytes<P>(nx, ny, nz, batch) +
+                          redi::flux_bytes<P>(nx, ny, nz, redi::tracer_group(batch, redi::cell_tuning().group));
+    const size_t need_a = redi::phase_a_scratch(nx, ny, nz);
+    e = s->ws.reserve(need_a > need_b ? need_a : need_b);
+    if (e != cudaSuccess) return cuda_fail(e, "redi_b200_step_host: scratch allocation");
+    cudaEvent_t start = hp.ev[0], done = hp.ev[1];
+    e = cudaEventRecord(start, caller);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hp.up, start, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hp.comp, start, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hp.down, start, 0);
+    if (doB && e == cudaSuccess) {  // per-face KhTr into the slots (ocean_redi.F90:981-987)
+        const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
+        if (use_ext) {
+            e = cudaMemcpyAsync(s->khtr_u, khtr_u_ext, nu * 8, cudaMemcpyDeviceToDevice, hp.comp);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(s->khtr_v, khtr_v_ext, nv * 8, cudaMemcpyDeviceToDevice, hp.comp);
+        } else {
+            e = fill(s->khtr_u, nu, s->khtr, hp.comp);
+            if (e == cudaSuccess) e = fill(s->khtr_v, nv, s->khtr, hp.comp);
+        }
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "redi_b200_step_host: set-up");
+    PhaseBInputs<P> in{};
+    in.nx = nx; in.ny = ny; in.nz = nz; in.nghost = grid->nghost; in.nxp = grid->nx_phys; in.nyp = grid->ny_phys;
+    for (int w = 0; w < 4; ++w) in.walls[w] = walls[w];
+    in.dt = dt; in.khtr = s->khtr; in.khtr_u = s->khtr_u; in.khtr_v = s->khtr_v;
+    in.dy_cu = metrics->dy_cu; in.dx_cv = metrics->dx_cv; in.idxCu = metrics->idxCu; in.idyCv = metrics->idyCv;
+    in.areaT = metrics->areaT; in.h = hp.h;
+    in.u = s->in_u<P>();
+    in.v = s->in_v<P>();
+    const double* th = hp.tin[ms->idx_temperature > 0 ? ms->idx_temperature - 1 : 0];
+    const double* sh = hp.tin[ms->idx_salinity > 0 ? ms->idx_salinity - 1 : 0];
+    int copied = 0;  // rows already on the device
+    for (int b = 0; b < nbands; ++b) {
+        const int j0 = (int)((long long)b * ny / nbands), j1 = (int)((long long)(b + 1) * ny / nbands);
+        const int need = j1 + 1 < ny ? j1 + 1 : ny;  // the band's cells read one row beyond it
+        cudaEvent_t up_b = hp.ev[2 + 2 * b], comp_b = hp.ev[3 + 2 * b];
+        if (need > copied) {
+            e = copy_rows(hp.h, ms->h_layer, nx, ny, nz, copied, need, cudaMemcpyHostToDevice, hp.up);
+            for (int t = 0; t < ntr && e == cudaSuccess; ++t)
+                e = copy_rows(hp.tin[t], ms->hTr[t], nx, ny, nz, copied, need, cudaMemcpyHostToDevice, hp.up);
+            copied = need;
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(up_b, hp.up);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(hp.comp, up_b, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "redi_b200_step_host: upload");
+        const redi::Band band{j0, j1};
+        if (doA) {
+            const int rc = run_phase_a<P>(nx, ny, nz, eos, hp.h, th, sh, metrics->wet_u, metrics->wet_v, s->out_u<P>(),
+                                          s->out_v<P>(), s->ws, hp.comp, band);
+            if (rc < 0) return rc;
+        }
+        if (doB) {
+            const int rc = run_phase_b<P>(in, ntr, hp.tout.data(), s->ws, hp.comp, hp.tin.data(), band);
+            if (rc < 0) return rc;
+            e = cudaEventRecord(comp_b, hp.comp);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(hp.down, comp_b, 0);
+            for (int t = 0; t < ntr && e == cudaSuccess; ++t)
+                e = copy_rows(ms->hTr[t], hp.tout[t], nx, ny, nz, j0, j1, cudaMemcpyDeviceToHost, hp.down);
+            if (e != cudaSuccess) return cuda_fail(e, "redi_b200_step_host: download");
+        }
+    }
+    cudaEvent_t last = hp.ev[2 + 2 * nbands];
+    e = cudaEventRecord(last, hp.comp);  // the last band's kernels, even without downloads
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hp.down, last, 0);
+    if (e == cudaSuccess) e = cudaEventRecord(done, hp.down);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(caller, done, 0);
+    return e == cudaSuccess ? REDI_B200_OK : cuda_fail(e, "redi_b200_step_host: join");
+}
+
+extern "C" {
+
+int redi_b200_step_host(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
+                        redi_b200* s, const redi_b200_state* ms, double dt, const double* khtr_u_ext,
+                        const double* khtr_v_ext, const redi_b200_bc* bc, int nbands, void* stream) {
+    if (!grid || !metrics || !eos || !s || !ms) return fail(REDI_B200_E_ARG, "redi_b200_step_host: NULL argument");
+    if (!s->is_init || !s->enable || !ms->h_layer) return REDI_B200_SKIPPED;
+    const int nx = grid->nx_total, ny = grid->ny_total, nz = ms->nz_ml;
+    if (s->nz_ml != nz) return REDI_B200_SKIPPED;
+    if (nx != s->nx_total || ny != s->ny_total)
+        return fail(REDI_B200_E_ARG, "redi_b200_step_host: grid extents differ from the handle's");
+    if (eos->variant == 3)
+        return fail(REDI_B200_E_UNSUPPORTED, "redi_b200_step_host: EOS variant 3 (TEOS-10) is reserved, not implemented");
+    if (eos->variant != 0 && eos->variant != 1 && eos->variant != 2 && eos->variant != 4)
+        return fail(REDI_B200_E_ARG, "redi_b200_step_host: unknown EOS variant (1 LINEAR, 2 WRIGHT_97, 4 ROQUET_SPV)");
+    if (nbands < 1) return fail(REDI_B200_E_ARG, "redi_b200_step_host: nbands must be >= 1");
+    if (nbands > ny) nbands = ny;
+    if (nbands > 64) nbands = 64;
+    // The two entry points' gates (ocean_redi.F90:585-593, 951-978), each on its own phase.
+    const bool ts = ms->idx_temperature > 0 && ms->idx_salinity > 0 && ms->hTr &&
+                    ms->idx_temperature <= ms->ntracers && ms->idx_salinity <= ms->ntracers;
+    if ((ms->idx_temperature > ms->ntracers || ms->idx_salinity > ms->ntracers) && ms->ntracers > 0)
+        return fail(REDI_B200_E_ARG, "redi_b200_step_host: temperature/salinity index outside the tracer table");
+    const bool use_ext = khtr_u_ext && khtr_v_ext;
+    const bool doA = ts;
+    const bool doB = ms->hTr && ms->ntracers > 0 && (use_ext || s->khtr > 0.0);
+    if (!doA && !doB) return REDI_B200_SKIPPED;
+    if (ms->ntracers > 0 && !ms->hTr) return fail(REDI_B200_E_ARG, "redi_b200_step_host: NULL tracer table");
+    for (int t = 0; t < ms->ntracers; ++t)
+        if (!ms->hTr[t]) return fail(REDI_B200_E_ARG, "redi_b200_step_host: NULL host tracer " + std::to_string(t + 1));
+    const double* need[] = {metrics->wet_u, metrics->wet_v, metrics->dy_cu, metrics->dx_cv, metrics->idxCu,
+                            metrics->idyCv, metrics->areaT};
+    for (const double* p : need)
+        if (!p || !aligned(p)) return fail(REDI_B200_E_ARG, "redi_b200_step_host: NULL or misaligned metric array");
+    int walls[4] = {1, 1, 1, 1};
+    if (bc) {
+        walls[0] = bc->west == REDI_B200_OBC_WALL;
+        walls[1] = bc->east == REDI_B200_OBC_WALL;
+        walls[2] = bc->south == REDI_B200_OBC_WALL;
+        walls[3] = bc->north == REDI_B200_OBC_WALL;
+    }
+    const redi::EosParams e{eos->variant, eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (s->precision == REDI_B200_MIXED)
+        return step_host_impl<redi::MixedPrec>(grid, metrics, e, s, ms, dt, doA, doB, walls, use_ext, khtr_u_ext,
+                                               khtr_v_ext, nbands, st);
+    return step_host_impl<redi::PlainPrec>(grid, metrics, e, s, ms, dt, doA, doB, walls, use_ext, khtr_u_ext,
+                                           khtr_v_ext, nbands, st);
 }
 
 // ---------------------------------------------------------------------------

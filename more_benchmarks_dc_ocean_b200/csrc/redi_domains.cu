@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <cstring>
 #include <new>
@@ -174,13 +175,13 @@ __global__ void __launch_bounds__(kThreads, OCC) k_domains(const DomainDev<P>* _
             const int t = (dir == 0 ? it.tile : it.tile - d.nu_tiles) * kThreads + tid;
             plain::sweep_item<P, LdCG, false>(d.sw, dir, t);
         } else if (st == S_RECON) {
-            plain::recon_item<2, P, LdCG>(d.rc, it.tile * kThreads + tid);
+            plain::recon_item<2, P, LdCG>(d.rc, it.tile * kThreads + tid, 0, d.rc.nx * d.rc.ny);
         } else {
             const int pair = (st - S_PAIR0) >> 1;
             if (((st - S_PAIR0) & 1) == 0) {
                 const int dir = it.tile < d.nu_tiles ? 0 : 1;
                 const int t = (dir == 0 ? it.tile : it.tile - d.nu_tiles) * kThreads + tid;
-                plain::flux_item<2, P, LdCG>(d.ff, dir, t, 2 * pair);
+                plain::flux_item<2, P, LdCG>(d.ff, dir, t, 2 * pair, INT_MAX);
             } else {
                 const int by = kThreads / bx;
                 const int i = (it.tile % d.gx) * bx + tid % bx;
@@ -408,6 +409,7 @@ int build(redi_b200_batch* b, int n, const redi_b200_domain* dom) {
         for (int t = 0; t < ntr; ++t) {
             d.rc.htr[t] = D.ms.hTr[t];
             cg.htr[t] = D.ms.hTr[t];
+            cg.htr_in[t] = D.ms.hTr[t];
         }
         const int npairs = (ntr + 1) / 2;
         const int nuf = (nx - 1) * ny, nvf = nx * (ny - 1);

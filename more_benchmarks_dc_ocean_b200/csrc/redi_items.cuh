@@ -481,12 +481,13 @@ __device__ __forceinline__ void store_ppm<MixedPrec>(PpmLayerF* p, const PpmLaye
 }
 
 template <int NT, class P, class LD>
-__device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid) {
+// gid enumerates (tracer group, column) over the columns [c0, c0 + nb).
+__device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid, int c0, int nb) {
     const int ncol = a.nx * a.ny;
     const int ngroups = (a.ntr + NT - 1) / NT;
-    if (gid >= ncol * ngroups) return;
-    const int col = gid % ncol;
-    const int g = gid / ncol;
+    if (gid >= nb * ngroups) return;
+    const int col = c0 + gid % nb;
+    const int g = gid / nb;
     const int tr0 = g * NT;
     const int nt = min(NT, a.ntr - tr0);
     const int nz = a.nz;
@@ -593,7 +594,9 @@ struct FluxOps<MixedPrec> {
 // skip) as one batch before any of them is used, so each sublayer costs one
 // memory round trip per tracer pair.
 template <int NT, class P, class LD>
-__device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, int t, int tr0) {
+// t enumerates the faces of direction dir; faces at t >= t_end (the end of the
+// launch's band, at most the direction's face count) are not this call's.
+__device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, int t, int tr0, int t_end) {
     using Ops = FluxOps<P>;
     using Raw = typename Ops::Raw;
     using He = typename P::He;
@@ -604,7 +607,7 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
     bool valid;
     if ((dir == 0 ? (nx - 1) * ny : nx * (ny - 1)) <= 0) return;  // no face 0 to stand in
     if (dir == 0) {  // Fortran faces I = 2..nx, excluding walls
-        valid = t < (nx - 1) * ny;
+        valid = t < min(t_end, (nx - 1) * ny);
         const int tt = valid ? t : 0;
         const int j = tt / (nx - 1), fi = 1 + tt % (nx - 1);
         const int I = fi + 1;
@@ -614,7 +617,7 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
         fo = fi + (nx + 1) * j;
         fstride = (size_t)(nx + 1) * ny;
     } else {  // Fortran faces J = 2..ny, excluding walls
-        valid = t < nx * (ny - 1);
+        valid = t < min(t_end, nx * (ny - 1));
         const int tt = valid ? t : 0;
         const int fj = 1 + tt / nx, i = tt % nx;
         const int J = fj + 1;
@@ -864,12 +867,13 @@ __device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, 
         for (int n = 0; n < NT; ++n) {
             if (n >= nt) break;
             double* __restrict__ out = a.htr[tr0 + n] + col;
+            const double* __restrict__ in = a.htr_in[tr0 + n] + col;  // == out for an in-place update
 #pragma unroll
             for (int c = 0; c < CH; ++c) {
                 const int k = k0 + c;
                 if (k < k1) {
                     const size_t o = (size_t)(nz - k) * ncol;
-                    out[o] = out[o] + dTr[n][c] * iaij;
+                    out[o] = in[o] + dTr[n][c] * iaij;
                 }
             }
         }

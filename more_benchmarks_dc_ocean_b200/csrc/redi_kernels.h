@@ -129,7 +129,8 @@ struct CellGatherArgsT {
     FaceInT<P> u, v;                  // only KoL / KoR are read
     const typename P::Flux* Fu;
     const typename P::Flux* Fv;
-    double* htr[kMaxTracers];
+    double* htr[kMaxTracers];         // updated tracers
+    const double* htr_in[kMaxTracers];  // pre-step tracers (the same arrays for an in-place update)
     int* err;                         // device error word (fluxes out of order), may be null
 };
 using CellGatherArgs = CellGatherArgsT<PlainPrec>;
@@ -194,14 +195,24 @@ struct CellTuning {
 CellTuning cell_tuning();
 void set_cell_tuning(const CellTuning& t);
 
-cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st);
+// A band of T-cell rows [row0, row1) of the domain (row1 < 0: to the last
+// row). A step restricted to a band touches the u faces of its rows, the v
+// faces between rows row0-1 .. row1 and the columns of rows row0-1 .. row1:
+// everything the band's cells need, and bands can be stepped one after
+// another with identical results when the tracers are read from pre-step
+// copies (CellGatherArgsT::htr_in).
+struct Band {
+    int row0 = 0, row1 = -1;
+};
+
+cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st, Band band = Band{});
 // Density and dSV/dT, dSV/dS at n points (T, S, p device arrays).
 cudaError_t launch_eos_points(const EosParams& e, int n, const double* T, const double* S, const double* p,
                               double* rho, double* dsv_dt, double* dsv_ds, cudaStream_t st);
 template <class P>
-cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st);
+cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st, Band band = Band{});
 template <class P>
 cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg,
-                           cudaStream_t st);
+                           cudaStream_t st, Band band = Band{});
 
 }  // namespace redi

@@ -165,6 +165,8 @@ int redi_b200_opt_launch_noalloc(const int* nx_, const int* ny_, const int* nz_,
     cg.areaT = areaT; cg.u = ff.u; cg.v = ff.v; cg.Fu = ff.Fu; cg.Fv = ff.Fv; cg.err = err;
     cg.htr[0] = t_htr;
     cg.htr[1] = s_htr;
+    cg.htr_in[0] = t_htr;
+    cg.htr_in[1] = s_htr;
     if (e == cudaSuccess) e = redi::launch_phase_b<redi::PlainPrec>(r, ff, cg, st);
     if (e != cudaSuccess) return set_error(REDI_B200_E_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     return REDI_B200_OK;

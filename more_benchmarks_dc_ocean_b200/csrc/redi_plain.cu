@@ -44,30 +44,39 @@ namespace plain {
 // Standalone kernels: one launch per stage, read-only inputs through the
 // non-coherent cache path.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col < a.nx * a.ny) column_state_item<LdNC>(a, col);
+// Face index ranges of one launch, per direction: faces lo[d] <= t < hi[d].
+struct FaceRange {
+    int lo[2], hi[2];
+};
+
+__global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a, int c0, int c1) {
+    const int col = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (col < c1) column_state_item<LdNC>(a, col);
 }
 
 template <class P>
-__global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgsT<P> a) {
-    sweep_item<P, LdNC, true>(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgsT<P> a, FaceRange r) {
+    const int d = blockIdx.y;
+    const int t = r.lo[d] + blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < r.hi[d]) sweep_item<P, LdNC, true>(a, d, t);
 }
 
 template <int NT, class P>
-__global__ void __launch_bounds__(128) k_tracer_recon(ReconArgsT<P> a) {
-    recon_item<NT, P, LdNC>(a, blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void __launch_bounds__(128) k_tracer_recon(ReconArgsT<P> a, int c0, int nb) {
+    recon_item<NT, P, LdNC>(a, blockIdx.x * blockDim.x + threadIdx.x, c0, nb);
 }
 
+// Every thread of the block reaches flux_item (its warp-wide votes need all lanes).
 template <int NT, class P>
-__global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0) {
-    flux_item<NT, P, LdNC>(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x, tr0);
+__global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0, FaceRange r) {
+    const int d = blockIdx.y;
+    flux_item<NT, P, LdNC>(a, d, r.lo[d] + blockIdx.x * blockDim.x + threadIdx.x, tr0, r.hi[d]);
 }
 
 template <int NT, int CH, class P>
-__global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgsT<P> a, int tr0, int fslot) {
-    gather_item<NT, CH, P, LdNC>(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y,
-                                 tr0, fslot);
+__global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgsT<P> a, int tr0, int fslot, int j0, int j1) {
+    const int j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (j < j1) gather_item<NT, CH, P, LdNC>(a, blockIdx.x * blockDim.x + threadIdx.x, j, tr0, fslot);
 }
 
 // The point EOS at n independent points, as the column state evaluates it at
@@ -93,11 +102,44 @@ __global__ void __launch_bounds__(128) k_eos_points(EosParams e, int n, const do
 // ---------------------------------------------------------------------------
 // Host launchers (stream-ordered, no synchronisation).
 // ---------------------------------------------------------------------------
-cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st) {
-    const int ncol = cs.nx * cs.ny;
-    launch_begin(K_COLUMN_STATE, st);
-    plain::k_column_state<<<(ncol + 127) / 128, 128, 0, st>>>(cs);
-    launch_end(K_COLUMN_STATE, st);
+namespace {
+
+// The index ranges a band of T-cell rows needs (see Band in redi_kernels.h).
+struct BandRanges {
+    int j0, j1;        // cell rows
+    int c0, c1;        // columns (rows j0-1 .. j1, clamped)
+    plain::FaceRange f;
+};
+
+BandRanges band_ranges(int nx, int ny, Band b) {
+    BandRanges r;
+    r.j0 = max(b.row0, 0);
+    r.j1 = b.row1 < 0 ? ny : min(b.row1, ny);
+    r.c0 = max(r.j0 - 1, 0) * nx;
+    r.c1 = min(r.j1 + 1, ny) * nx;
+    r.f.lo[0] = r.j0 * (nx - 1);  // u faces of rows j0 .. j1-1
+    r.f.hi[0] = r.j1 * (nx - 1);
+    const int f0 = max(r.j0, 1), f1 = min(r.j1, ny - 1);  // v faces between rows f-1 and f, f0 <= f <= f1
+    r.f.lo[1] = (f0 - 1) * nx;
+    r.f.hi[1] = f1 >= f0 ? f1 * nx : r.f.lo[1];
+    if (r.j1 <= r.j0) r.c1 = r.c0, r.f.hi[0] = r.f.lo[0], r.f.hi[1] = r.f.lo[1];
+    return r;
+}
+
+unsigned face_blocks(const plain::FaceRange& f) {
+    const int n = max(f.hi[0] - f.lo[0], f.hi[1] - f.lo[1]);
+    return (unsigned)((max(n, 0) + 127) / 128);
+}
+
+}  // namespace
+
+cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st, Band band) {
+    const BandRanges r = band_ranges(cs.nx, cs.ny, band);
+    if (r.c1 > r.c0) {
+        launch_begin(K_COLUMN_STATE, st);
+        plain::k_column_state<<<(r.c1 - r.c0 + 127) / 128, 128, 0, st>>>(cs, r.c0, r.c1);
+        launch_end(K_COLUMN_STATE, st);
+    }
     return cudaGetLastError();
 }
 
@@ -111,38 +153,46 @@ cudaError_t launch_eos_points(const EosParams& e, int n, const double* T, const 
 }
 
 template <class P>
-cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st) {
-    const int nface = max((sw.nx - 1) * sw.ny, sw.nx * (sw.ny - 1));
-    if (nface > 0) {
+cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st, Band band) {
+    const BandRanges r = band_ranges(sw.nx, sw.ny, band);
+    const unsigned nb = face_blocks(r.f);
+    if (nb > 0) {
         const int kid = P::kMixed ? K_MIXED_SWEEP : K_NEUTRAL_SWEEP;
-        dim3 grid((nface + 127) / 128, 2);
         launch_begin(kid, st);
-        plain::k_neutral_sweep<P><<<grid, 128, 0, st>>>(sw);
+        plain::k_neutral_sweep<P><<<dim3(nb, 2), 128, 0, st>>>(sw, r.f);
         launch_end(kid, st);
     }
     return cudaGetLastError();
 }
 
 template <int NT, class P>
-static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg, int tr0, int nface,
-                               const CellTuning& tune, cudaStream_t st) {
+static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg, int tr0,
+                               const BandRanges& r, const CellTuning& tune, cudaStream_t st) {
     const dim3 block(tune.bx, tune.by);
-    const dim3 cgrid((cg.nx + tune.bx - 1) / tune.bx, (cg.ny + tune.by - 1) / tune.by);
-    if (nface > 0) {
+    const dim3 cgrid((cg.nx + tune.bx - 1) / tune.bx, (r.j1 - r.j0 + tune.by - 1) / tune.by);
+    const unsigned nb = face_blocks(r.f);
+    if (nb > 0) {
         const int kid = P::kMixed ? K_MIXED_FLUX : K_FACE_FLUX;
         launch_begin(kid, st);
-        plain::k_face_flux<NT, P><<<dim3((nface + 127) / 128, 2), 128, 0, st>>>(ff, tr0);
+        plain::k_face_flux<NT, P><<<dim3(nb, 2), 128, 0, st>>>(ff, tr0, r.f);
         launch_end(kid, st);
     }
+    if (cgrid.y == 0) return;
     // The gather folds tracer pairs (its per-layer sums live in registers);
     // a group's pairs read consecutive slots of the flux buffer.
     for (int g = 0; g < NT; g += 2) {
         if (tr0 + g >= cg.ntr) break;
         launch_begin(K_CELL_UPDATE, st);
         switch (tune.chunk) {
-            case 4: plain::k_cell_gather<NT < 2 ? NT : 2, 4, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g); break;
-            case 16: plain::k_cell_gather<NT < 2 ? NT : 2, 16, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g); break;
-            default: plain::k_cell_gather<NT < 2 ? NT : 2, 8, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g); break;
+            case 4:
+                plain::k_cell_gather<NT < 2 ? NT : 2, 4, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g, r.j0, r.j1);
+                break;
+            case 16:
+                plain::k_cell_gather<NT < 2 ? NT : 2, 16, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g, r.j0, r.j1);
+                break;
+            default:
+                plain::k_cell_gather<NT < 2 ? NT : 2, 8, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g, r.j0, r.j1);
+                break;
         }
         launch_end(K_CELL_UPDATE, st);
     }
@@ -150,36 +200,36 @@ static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT
 
 template <class P>
 cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg,
-                           cudaStream_t st) {
-    const int ncol = rc.nx * rc.ny;
+                           cudaStream_t st, Band band) {
+    const BandRanges r = band_ranges(rc.nx, rc.ny, band);
     // Reconstruct in groups of two tracers (register window of 2 scalars).
-    {
+    if (r.c1 > r.c0) {
         const int ngroups = (rc.ntr + 1) / 2;
-        const long long n = (long long)ncol * ngroups;
+        const int nb = r.c1 - r.c0;
+        const long long n = (long long)nb * ngroups;
         const int kid = P::kMixed ? K_MIXED_RECON : K_TRACER_RECON;
         launch_begin(kid, st);
-        plain::k_tracer_recon<2, P><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc);
+        plain::k_tracer_recon<2, P><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc, r.c0, nb);
         launch_end(kid, st);
     }
     const CellTuning tune = cell_tuning();
-    const int nface = max((ff.nx - 1) * ff.ny, ff.nx * (ff.ny - 1));
     const int group = tracer_group(ff.ntr, tune.group);
     for (int tr0 = 0; tr0 < ff.ntr; tr0 += group) {
         switch (group) {
-            case 8: launch_flux_gather<8, P>(ff, cg, tr0, nface, tune, st); break;
-            case 4: launch_flux_gather<4, P>(ff, cg, tr0, nface, tune, st); break;
-            case 2: launch_flux_gather<2, P>(ff, cg, tr0, nface, tune, st); break;
-            default: launch_flux_gather<1, P>(ff, cg, tr0, nface, tune, st); break;
+            case 8: launch_flux_gather<8, P>(ff, cg, tr0, r, tune, st); break;
+            case 4: launch_flux_gather<4, P>(ff, cg, tr0, r, tune, st); break;
+            case 2: launch_flux_gather<2, P>(ff, cg, tr0, r, tune, st); break;
+            default: launch_flux_gather<1, P>(ff, cg, tr0, r, tune, st); break;
         }
     }
     return cudaGetLastError();
 }
 
-template cudaError_t launch_sweep<PlainPrec>(const SweepArgsT<PlainPrec>&, cudaStream_t);
-template cudaError_t launch_sweep<MixedPrec>(const SweepArgsT<MixedPrec>&, cudaStream_t);
+template cudaError_t launch_sweep<PlainPrec>(const SweepArgsT<PlainPrec>&, cudaStream_t, Band);
+template cudaError_t launch_sweep<MixedPrec>(const SweepArgsT<MixedPrec>&, cudaStream_t, Band);
 template cudaError_t launch_phase_b<PlainPrec>(const ReconArgsT<PlainPrec>&, const FaceFluxArgsT<PlainPrec>&,
-                                               const CellGatherArgsT<PlainPrec>&, cudaStream_t);
+                                               const CellGatherArgsT<PlainPrec>&, cudaStream_t, Band);
 template cudaError_t launch_phase_b<MixedPrec>(const ReconArgsT<MixedPrec>&, const FaceFluxArgsT<MixedPrec>&,
-                                               const CellGatherArgsT<MixedPrec>&, cudaStream_t);
+                                               const CellGatherArgsT<MixedPrec>&, cudaStream_t, Band);
 
 }  // namespace redi

@@ -409,6 +409,32 @@ def to_device(p, device="cuda", tracers: Optional[Sequence[np.ndarray]] = None) 
         bc=OceanBC(wall(ww), wall(we), wall(ws), wall(wn)), dt=p.dt)
 
 
+def _hptr(t) -> int:
+    import torch
+
+    assert isinstance(t, torch.Tensor) and not t.is_cuda and t.dtype == torch.float64 and t.is_contiguous(), t
+    return t.data_ptr()
+
+
+def redi_step_host(grid: HGrid, metrics: OceanMetrics, eos: OceanEos, this: OceanRedi, ms_host: MultilayerState,
+                   dt: float, khtr_u_ext=None, khtr_v_ext=None, bc: Optional[OceanBC] = None, nbands: int = 8,
+                   stream=None) -> int:
+    """redi_calc_coeffs + redi_apply_flux on a host-resident state (h and tracers are CPU float64
+    tensors, page-locked for overlap), pipelined over ``nbands`` row bands; stream-ordered."""
+    if not this.is_init:
+        return SKIPPED
+    L = lib()
+    L.redi_b200_step_host.argtypes = [C.POINTER(_Grid), C.POINTER(_Metrics), C.POINTER(_Eos), C.c_void_p,
+                                      C.POINTER(_State), C.c_double, C.c_void_p, C.c_void_p, C.POINTER(_BC),
+                                      C.c_int, C.c_void_p]
+    arr = (C.c_void_p * max(1, len(ms_host.tracers)))(*[_hptr(t) for t in ms_host.tracers])
+    st = _State(ms_host.nz_ml, ms_host.idx_temperature, ms_host.idx_salinity, len(ms_host.tracers),
+                _hptr(ms_host.h_layer), C.cast(arr, C.POINTER(C.c_void_p)) if ms_host.tracers else None)
+    return _check(L.redi_b200_step_host(C.byref(grid._c()), C.byref(metrics._c()), C.byref(eos._c()), this._h,
+                                        C.byref(st), float(dt), _ptr(khtr_u_ext), _ptr(khtr_v_ext),
+                                        C.byref(bc._c()) if bc is not None else None, int(nbands), _stream(stream)))
+
+
 def eos_points(eos: OceanEos, T, S, p, stream=None):
     """eos_density_point + eos_specvol_derivs (redi/ocean_eos.F90:450-546) at every point of the
     float64 CUDA tensors T, S, p (Pa); returns (rho, dsv_dt, dsv_ds) tensors."""
