@@ -22,10 +22,21 @@ mkdir -p "$OUT"
 FLAGS=(-O3 -gencode arch=compute_100a,code=sm_100a -fmad=false -I"$REF/common" -I"$REF/redi"
        --compiler-options -fPIC -DMODEL_NZ_STACK_MAX=128 -DWITH_CUDA)
 LIB="$OUT/libredi_refcuda.so"
-if [[ -f "$LIB" && "$LIB" -nt "$REF/redi/redi_kernel.cu" && "$LIB" -nt "$REF/redi/opt_kernel.cu" && "$LIB" -nt "$0" ]]; then
+# The same launchers built with the reference's own flags only (FMA contraction
+# on, as its Makefile builds them), for timing the reference on this GPU
+# (oracle/time_reference_cuda.py); not used for parity.
+NATIVE="$OUT/libredi_refcuda_native.so"
+if [[ -f "$LIB" && -f "$NATIVE" && "$LIB" -nt "$REF/redi/redi_kernel.cu" && "$LIB" -nt "$REF/redi/opt_kernel.cu" \
+      && "$LIB" -nt "$0" && "$NATIVE" -nt "$0" ]]; then
   exit 0
 fi
 "$NVCC" "${FLAGS[@]}" -c "$REF/redi/redi_kernel.cu" -o "$OUT/redi_kernel.o"
 "$NVCC" "${FLAGS[@]}" -c "$REF/redi/opt_kernel.cu" -o "$OUT/opt_kernel.o"
 "$NVCC" -gencode arch=compute_100a,code=sm_100a -shared -o "$LIB" "$OUT/redi_kernel.o" "$OUT/opt_kernel.o"
 echo "built $LIB"
+NFLAGS=(-O3 -gencode arch=compute_100a,code=sm_100a -I"$REF/common" -I"$REF/redi"
+        --compiler-options -fPIC -DMODEL_NZ_STACK_MAX=128 -DWITH_CUDA)
+"$NVCC" "${NFLAGS[@]}" -c "$REF/redi/redi_kernel.cu" -o "$OUT/redi_kernel_native.o"
+"$NVCC" "${NFLAGS[@]}" -c "$REF/redi/opt_kernel.cu" -o "$OUT/opt_kernel_native.o"
+"$NVCC" -gencode arch=compute_100a,code=sm_100a -shared -o "$NATIVE" "$OUT/redi_kernel_native.o" "$OUT/opt_kernel_native.o"
+echo "built $NATIVE"
