@@ -52,7 +52,8 @@ sys.path.insert(0, ROOT)
 METRIC = "Redi tracer-cell updates/s, HBM GB/s; mixed+batched vs FP64 plain, 1 B200"
 UNIT = "tracer-cell updates/s"
 KERNEL_NAMES = ["k_column_state", "k_neutral_sweep", "k_tracer_recon", "k_cell_gather", "k_face_flux",
-                "k_mixed_recon", "k_mixed_flux", "k_mixed_sweep", "k_domain_persistent", "aux"]
+                "k_mixed_recon", "k_mixed_flux", "k_mixed_sweep", "k_domain_persistent", "aux",
+                "k_meke_column", "k_meke_del2", "k_meke_lateral"]
 NKERN = len(KERNEL_NAMES)
 FALLBACK_HBM_GBS = 6650.0
 
@@ -735,13 +736,252 @@ def _e2e(args, p, dp, redi, ex, st, dist, dev, world):
             "host_memory": "pinned", "path": path, "band_candidates_ms": band_ms}
 
 
+# ---------------------------------------------------------------------------
+# MEKE step (meke_step_ext): the diffusivity producer
+# ---------------------------------------------------------------------------
+MEKE_METRIC = "MEKE step column-steps/s (meke_step_ext, gabight_sph_meke_v100 configuration), 1 B200"
+MEKE_UNIT = "column-steps/s"
+
+
+def _meke_problem(config: str):
+    from more_benchmarks_dc_ocean_b200 import meke_inputs as MI
+
+    if config == "meke":  # the reference's benchmark: 473 x 297 points, 3 ghosts, 30 layers
+        return MI.reference_ic()
+    return MI.reference_ic(1440, 1080, 75, nghost=2)  # meke_c1: the Redi config-1 grid
+
+
+def meke_bytes(nx: int, ny: int, nz: int):
+    """Algorithmic bytes of the MEKE kernels per step at the gabight configuration (pass A, pass B).
+
+    Pass A reads h and rho (nz layers each), areaT, meke, gm_src, ke_diss_ext, u_bbl2 and writes
+    the zeroed SN faces, rd, ke_diss, depth, mass, 1/mass, both structure factors, Lmix, the source
+    and the post-drag energy. Pass B reads the post-drag energy, mass, 1/area, 1/mass, the bottom
+    factor, u_bbl2, the barotropic factor, Lmix and the four face metrics, and writes meke,
+    kh_diff, ku and the two face fluxes."""
+    nt, nu, nv = nx * ny, (nx + 1) * ny, nx * (ny + 1)
+    a = 8 * (2 * nz * nt + 5 * nt + 10 * nt + nu + nv)
+    b = 8 * (8 * nt + 2 * nu + 2 * nv + 3 * nt + nu + nv)
+    return float(a), float(b)
+
+
+def _ncu_traffic_tag(tag: str) -> dict:
+    out = {}
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return out
+    for fn in os.listdir(d):
+        if fn.endswith(".md"):
+            for line in open(os.path.join(d, fn)):
+                m = re.match(rf"^traffic_bytes_per_launch_{tag}:\s*(\w+)\s*=\s*([\d.eE+]+)", line.strip())
+                if m:
+                    out[m.group(1)] = float(m.group(2))
+    return out
+
+
+def meke_cpu_sample(p, target_s: float, nsteps: int = 0, warmup: int = 0):
+    """The MEKE oracle on the whole domain, all host threads; returns (column-steps/s, info)."""
+    from oracle import meke_oracle as MO
+
+    threads = len(os.sched_getaffinity(0))
+    q = p.copy()
+    t0 = time.perf_counter()
+    MO.step(q, 1)
+    probe = max(time.perf_counter() - t0, 1e-4)
+    n = nsteps or int(max(3, min(400, target_s / probe)))
+    times = []
+    for s in range(warmup + n):
+        t0 = time.perf_counter()
+        MO.step(q, 1)
+        if s >= warmup:
+            times.append(time.perf_counter() - t0)
+    t = min(times)
+    return p.nx * p.ny / t, {"cores": threads, "t_step_s": t, "steps": n,
+                             "sample": f"{p.nx}x{p.ny}x{p.nz} ({p.name}), whole domain, min of {n} step(s)"}
+
+
+def _meke_config_block(p, world):
+    return {"workload": f"MEKE step {p.nx}x{p.ny}x{p.nz} (arrays incl. ghosts), gabight_sph_meke_v100 "
+                        f"(gmcoeff 0.9, khcoeff 1, cdrag 2.5e-3, kh 100)" + (f", {world} replicas" if world > 1 else ""),
+            "grid": [p.nx, p.ny, p.nz], "dt_s": p.config["dt"],
+            "l2": "L2 flushed (256 MB write) before every timed step",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"}
+
+
+def run_meke_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    p = _meke_problem(args.config)
+    budget = 120.0
+    per = max(1.0, budget / max(1, args.steps + args.warmup))
+    val, info = meke_cpu_sample(p, per, nsteps=args.steps, warmup=args.warmup)
+    print(json.dumps({
+        "impl": "reference", "metric": MEKE_METRIC, "value": val, "unit": MEKE_UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": info["t_step_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": _meke_config_block(p, world),
+        "cpu_baseline": {"value": val, "unit": MEKE_UNIT, "cores": info["cores"], "kind": "port",
+                         "sample": info["sample"]},
+        "e2e": {"value": val, "unit": MEKE_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU path (meke_step_ext restated in C++, OpenMP over all host cores); the Fortran "
+                "build itself needs a Fortran compiler, absent on this image"}), flush=True)
+    return 0
+
+
+def run_meke(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+
+    from more_benchmarks_dc_ocean_b200 import ocean_meke as M
+    from more_benchmarks_dc_ocean_b200 import ocean_redi as R
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:  # independent replicas: the step has no exchange of its own
+        import torch.distributed as dist  # noqa: F811
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    p = _meke_problem(args.config)
+    d = M.to_device(p, dev)
+    L = M.lib()
+    RL = R.lib()
+    RL.redi_b200_launch_count.restype = C.c_ulonglong
+    RL.redi_b200_launch_count.argtypes = [C.c_int]
+    h = C.c_void_p()
+    assert L.meke_b200_create(p.nx, p.ny, p.nz, C.byref(h)) == 0, M.last_error()
+    margs = M.make_args(p.nx, p.ny, p.nz, d, p.config)
+    del2 = C.c_void_p(d["del2"].data_ptr())
+    st = torch.cuda.current_stream()
+    sp = C.c_void_p(st.cuda_stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB, twice the L2
+
+    def step():
+        rc = L.meke_b200_step(h, C.byref(margs), del2, sp)
+        if rc != 0:
+            raise RuntimeError(M.last_error())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def timed(nsteps, profile=False):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+        if profile:
+            RL.redi_b200_profile_begin()
+        n0 = RL.redi_b200_launch_count(-1)
+        for i in range(nsteps):
+            flush.fill_(float(i))  # evict the previous step's fields from L2
+            ev[i][0].record(st)
+            step()
+            ev[i][1].record(st)
+        torch.cuda.synchronize()
+        n1 = RL.redi_b200_launch_count(-1)
+        kt = (C.c_double * NKERN)()
+        kc = (C.c_ulonglong * NKERN)()
+        if profile:
+            RL.redi_b200_profile_end(kt, kc, NKERN)
+        return sum(a.elapsed_time(b) for a, b in ev) / nsteps, int(n1 - n0), kt, kc
+
+    clocks = ClockSampler(_uuid(local_rank))
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ms, launches, _, _ = timed(args.steps)
+    barrier()
+    clk = clocks.stop()
+    ms_all = _max_over_ranks(ms, dist, dev)
+    value = p.nx * p.ny * world / (ms_all * 1e-3)
+
+    # per-kernel device times (events around each launch: a separate pass, as they cut the programmatic edge)
+    _, _, kt, kc = timed(args.steps, profile=True)
+    kern = {KERNEL_NAMES[k]: {"ms_total": kt[k], "launches": int(kc[k]), "ms_per_launch": kt[k] / kc[k]}
+            for k in range(NKERN) if kc[k]}
+    bytes_a, bytes_b = meke_bytes(p.nx, p.ny, p.nz)
+    peak, peak_kind = _peaks()
+    ka, kb = 10, 12
+    ta, tb = kt[ka] / kc[ka] * 1e-3, kt[kb] / kc[kb] * 1e-3
+    achieved = bytes_a / ta / 1e9
+    traffic = _ncu_traffic_tag("meke" if args.config == "meke" else "meke_c1").get("k_meke_column")
+
+    # warm L2: back-to-back steps, no flush (the reference workload's fields fit in the 126 MB L2)
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0.record(st)
+    for _ in range(args.steps):
+        step()
+    w1.record(st)
+    torch.cuda.synchronize()
+    warm_ms = w0.elapsed_time(w1) / args.steps
+
+    e2e = None
+    if not args.no_e2e:
+        ins = ("h_layer", "rho_layer", "meke", "kh_diff", "gm_src", "ke_diss_ext", "u_bbl2")
+        outs = ("meke", "kh_diff", "ku")
+        host = {k: torch.from_numpy(np.ascontiguousarray(p.arrays[k])).pin_memory() for k in set(ins + outs)}
+
+        def e2e_step():
+            for k in ins:
+                d[k].copy_(host[k], non_blocking=True)
+            step()
+            for k in outs:
+                host[k].copy_(d[k], non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        for _ in range(args.steps):
+            e2e_step()
+        b.record(st)
+        torch.cuda.synchronize()
+        ems = _max_over_ranks(a.elapsed_time(b) / args.steps, dist, dev)
+        e2e = {"value": p.nx * p.ny * world / (ems * 1e-3), "unit": MEKE_UNIT, "ms_per_step": ems,
+               "h2d_bytes_per_step": int(sum(host[k].numel() * 8 for k in ins)),
+               "d2h_bytes_per_step": int(sum(host[k].numel() * 8 for k in outs)), "host_memory": "pinned",
+               "path": "meke_b200_step with its inputs copied up and meke / kh_diff / ku copied back every step"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, info = meke_cpu_sample(p, args.cpu_seconds)
+        cpu = {"value": v, "unit": MEKE_UNIT, "cores": info["cores"], "kind": "port", "sample": info["sample"]}
+
+    if rank == 0:
+        print(json.dumps({
+            "metric": MEKE_METRIC, "value": value, "unit": MEKE_UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_all, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": _meke_config_block(p, world),
+            "roofline": {"bound": "hbm", "kernel": "k_meke_column", "achieved": achieved, "peak": peak,
+                         "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": bytes_a},
+            "step_roofline": {"algorithmic_bytes_per_step": bytes_a + bytes_b,
+                              "achieved_gbs": (bytes_a + bytes_b) / (ms_all * 1e-3) / 1e9,
+                              "frac": (bytes_a + bytes_b) / (ms_all * 1e-3) / 1e9 / peak,
+                              "pass_b_gbs": bytes_b / tb / 1e9},
+            "kernels": kern, "warm_l2_ms_per_step": warm_ms, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": launches}), flush=True)
+    L.meke_b200_destroy(h)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="config1", choices=["config0", "config1", "config3", "config4"])
+    ap.add_argument("--config", default="config1",
+                    choices=["config0", "config1", "config3", "config4", "meke", "meke_c1"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: a generated domain of that size instead of --config")
     ap.add_argument("--no-e2e", action="store_true")
@@ -754,7 +994,11 @@ def main():
         ap.error("--warmup must be >= 3")
     rank, world, local_rank = _rank_env()
     if args.impl == "reference":
+        if args.config.startswith("meke"):
+            return run_meke_reference(args, rank, world)
         return run_reference(args, rank, world)
+    if args.config.startswith("meke"):
+        return run_meke(args, rank, world, local_rank)
     if args.config == "config4":
         return run_domains(args, rank, world, local_rank)
     return run_b200(args, rank, world, local_rank)

@@ -289,6 +289,9 @@ void launch_begin(int kid, cudaStream_t st) {
     cudaEventRecord(r.a, st);
     g_prof.recs.push_back(r);
 }
+void count_launches(int kid, unsigned long long n) {
+    __atomic_add_fetch(&g_prof.launches[kid], n, __ATOMIC_RELAXED);
+}
 void launch_end(int kid, cudaStream_t st) {
     std::lock_guard<std::mutex> lock(g_prof.mu);
     if (!g_prof.active) return;

@@ -174,7 +174,10 @@ enum KernelId : int {
     K_MIXED_SWEEP = 7,
     K_DOMAIN_PERSISTENT = 8,
     K_AUX = 9,
-    K_NUM = 10
+    K_MEKE_COLUMN = 10,   // MEKE pass A
+    K_MEKE_DEL2 = 11,     // MEKE biharmonic Laplacian
+    K_MEKE_LATERAL = 12,  // MEKE pass B
+    K_NUM = 13
 };
 
 // Sets the message redi_b200_last_error() returns on the calling thread.
@@ -185,6 +188,9 @@ void set_last_error(const std::string& msg);
 // around it on the launching stream.
 void launch_begin(int kid, cudaStream_t st);
 void launch_end(int kid, cudaStream_t st);
+// Adds n launches of kernel kid to the counter without timing them (CUDA graph
+// replays, whose launches happen inside the graph).
+void count_launches(int kid, unsigned long long n);
 
 // Launch shape of Phase B: the cell gather's bx x by tile of columns per
 // block (bx * by <= 128) and vertical chunk (layers per pass, 4, 8 or 16),

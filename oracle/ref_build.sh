@@ -1,14 +1,20 @@
 #!/usr/bin/env bash
-# Builds the reference's own CUDA launchers — redi/redi_kernel.cu
-# (`redi_cuda_launch_`) and redi/opt_kernel.cu (`redi_opt_launch`) — from the
-# reference sources where they lie, into oracle/_ref/libredi_refcuda.so.
-# Test infrastructure only: used on a B200 to generate the golden vectors that
-# pin the CPU oracle (tests/golden/make_golden.py).
+# Builds the reference's own CUDA launchers from the reference sources where
+# they lie, into oracle/_ref/. Test infrastructure only: used on a B200 to
+# generate the golden vectors that pin the CPU oracles (tests/golden/) and to
+# time the reference's CUDA beside this repository's kernels.
 #
-# Built exactly as the reference's Makefile builds them (redi/Makefile:57-63:
-# -O3, -I../common, -DMODEL_NZ_STACK_MAX=128 -DWITH_CUDA) except for two flags:
-# the target is sm_100a, and FMA contraction is off (-fmad=false) so the
-# result is the IEEE sequence of the source, comparable bit for bit.
+#   libredi_refcuda.so   redi/redi_kernel.cu (`redi_cuda_launch_`) and
+#                        redi/opt_kernel.cu (`redi_opt_launch`)
+#   libmeke_refcuda.so   meke/meke_kernel.cu (`meke_cuda_launch`) and
+#                        meke/opt_kernel.cu (`meke_opt_launch`)
+#
+# Built as the reference's Makefiles build them (redi/Makefile:57-63: -O3,
+# -I../common, -DMODEL_NZ_STACK_MAX=128 -DWITH_CUDA; meke/Makefile CUFLAGS:
+# -O3, -I../common -I.) except for two flags: the target is sm_100a, and FMA
+# contraction is off (-fmad=false) so the result is the IEEE sequence of the
+# source, comparable bit for bit. The *_native.so twins keep the reference's
+# own flags (FMA contraction on) and are used only for timing.
 set -euo pipefail
 REF="${REDI_REFERENCE_DIR:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -18,25 +24,37 @@ if [[ ! -f "$REF/redi/redi_kernel.cu" ]]; then
   exit 0
 fi
 NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
+ARCH=(-gencode arch=compute_100a,code=sm_100a)
 mkdir -p "$OUT"
-FLAGS=(-O3 -gencode arch=compute_100a,code=sm_100a -fmad=false -I"$REF/common" -I"$REF/redi"
-       --compiler-options -fPIC -DMODEL_NZ_STACK_MAX=128 -DWITH_CUDA)
-LIB="$OUT/libredi_refcuda.so"
-# The same launchers built with the reference's own flags only (FMA contraction
-# on, as its Makefile builds them), for timing the reference on this GPU
-# (oracle/time_reference_cuda.py); not used for parity.
-NATIVE="$OUT/libredi_refcuda_native.so"
-if [[ -f "$LIB" && -f "$NATIVE" && "$LIB" -nt "$REF/redi/redi_kernel.cu" && "$LIB" -nt "$REF/redi/opt_kernel.cu" \
-      && "$LIB" -nt "$0" && "$NATIVE" -nt "$0" ]]; then
-  exit 0
+
+# build_pair <name> <srcdir> <extra flags...> -- <sources...>
+build_pair() {
+  local name="$1" dir="$2"; shift 2
+  local extra=()
+  while [[ "$1" != "--" ]]; do extra+=("$1"); shift; done
+  shift
+  local srcs=("$@")
+  local lib="$OUT/lib${name}_refcuda.so" native="$OUT/lib${name}_refcuda_native.so"
+  local fresh=1
+  for s in "${srcs[@]}"; do
+    [[ -f "$lib" && -f "$native" && "$lib" -nt "$dir/$s" && "$lib" -nt "$0" && "$native" -nt "$0" ]] || fresh=0
+  done
+  [[ $fresh == 1 ]] && return 0
+  local objs=() nobjs=()
+  for s in "${srcs[@]}"; do
+    local b="${s%.cu}"
+    "$NVCC" -O3 "${ARCH[@]}" -fmad=false -I"$REF/common" -I"$dir" --compiler-options -fPIC "${extra[@]}" \
+      -c "$dir/$s" -o "$OUT/${name}_${b}.o"
+    "$NVCC" -O3 "${ARCH[@]}" -I"$REF/common" -I"$dir" --compiler-options -fPIC "${extra[@]}" \
+      -c "$dir/$s" -o "$OUT/${name}_${b}_native.o"
+    objs+=("$OUT/${name}_${b}.o"); nobjs+=("$OUT/${name}_${b}_native.o")
+  done
+  "$NVCC" "${ARCH[@]}" -shared -o "$lib" "${objs[@]}"
+  "$NVCC" "${ARCH[@]}" -shared -o "$native" "${nobjs[@]}"
+  echo "built $lib $native"
+}
+
+build_pair redi "$REF/redi" -DMODEL_NZ_STACK_MAX=128 -DWITH_CUDA -- redi_kernel.cu opt_kernel.cu
+if [[ -f "$REF/meke/meke_kernel.cu" ]]; then
+  build_pair meke "$REF/meke" -- meke_kernel.cu opt_kernel.cu
 fi
-"$NVCC" "${FLAGS[@]}" -c "$REF/redi/redi_kernel.cu" -o "$OUT/redi_kernel.o"
-"$NVCC" "${FLAGS[@]}" -c "$REF/redi/opt_kernel.cu" -o "$OUT/opt_kernel.o"
-"$NVCC" -gencode arch=compute_100a,code=sm_100a -shared -o "$LIB" "$OUT/redi_kernel.o" "$OUT/opt_kernel.o"
-echo "built $LIB"
-NFLAGS=(-O3 -gencode arch=compute_100a,code=sm_100a -I"$REF/common" -I"$REF/redi"
-        --compiler-options -fPIC -DMODEL_NZ_STACK_MAX=128 -DWITH_CUDA)
-"$NVCC" "${NFLAGS[@]}" -c "$REF/redi/redi_kernel.cu" -o "$OUT/redi_kernel_native.o"
-"$NVCC" "${NFLAGS[@]}" -c "$REF/redi/opt_kernel.cu" -o "$OUT/opt_kernel_native.o"
-"$NVCC" -gencode arch=compute_100a,code=sm_100a -shared -o "$NATIVE" "$OUT/redi_kernel_native.o" "$OUT/opt_kernel_native.o"
-echo "built $NATIVE"
