@@ -118,18 +118,45 @@ def kernel_bytes(p, kid: int, precision: str = "fp64") -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons of one GPU, sampled every 200 ms."""
+    """Clocks and throttle reasons of one GPU during a timed region: nvidia-smi every 200 ms, and an
+    NVML poller every 2 ms for regions shorter than nvidia-smi's period (read-only queries)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # nvmlClocksEventReason* bits
+    NVML_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, uuid: str | None):
         self.uuid = uuid
         self.proc = None
         self.path = None
+        self.nvml = []
+        self._stop = None
+        self._thread = None
+
+    def _poll_nvml(self):
+        try:
+            import pynvml as N
+
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByUUID(self.uuid) if self.uuid else N.nvmlDeviceGetHandleByIndex(0)
+            mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                rs = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.nvml.append((sm, mx, rs))
+                self._stop.wait(0.002)
+            N.nvmlShutdown()
+        except Exception:
+            pass
 
     def start(self):
+        import threading
+
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._poll_nvml, daemon=True)
+        self._thread.start()
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -140,30 +167,43 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _nvml_summary(self) -> dict:
+        sm = [x[0] for x in self.nvml]
+        reasons = sorted({n for x in self.nvml for n, b in self.NVML_BITS.items() if x[2] & b})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(x[1] for x in self.nvml), "reasons": reasons,
+                "samples": len(sm), "source": "nvml, 2 ms"}
+
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
+        if self._stop is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
         rows = []
-        with open(self.path) as f:
-            for line in f:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.path)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+            os.unlink(self.path)
         if not rows:
+            if self.nvml:
+                return self._nvml_summary()
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         pw = [float(r[3]) for r in rows if re.match(r"^[\d.]+$", r[3])]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+               "power_w_max": max(pw) if pw else None, "reasons": reasons, "samples": len(rows)}
+        if self.nvml:
+            out["nvml"] = self._nvml_summary()
+        return out
 
 
 def _ncu_traffic() -> dict:
@@ -804,7 +844,7 @@ def _meke_config_block(p, world):
     return {"workload": f"MEKE step {p.nx}x{p.ny}x{p.nz} (arrays incl. ghosts), gabight_sph_meke_v100 "
                         f"(gmcoeff 0.9, khcoeff 1, cdrag 2.5e-3, kh 100)" + (f", {world} replicas" if world > 1 else ""),
             "grid": [p.nx, p.ny, p.nz], "dt_s": p.config["dt"],
-            "l2": "L2 flushed (256 MB write) before every timed step",
+            "l2": "L2 evicted before every timed step: 256 MB write, then 256 MB read (cold, clean L2)",
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"}
 
 
@@ -856,7 +896,15 @@ def run_meke(args, rank, world, local_rank):
     del2 = C.c_void_p(d["del2"].data_ptr())
     st = torch.cuda.current_stream()
     sp = C.c_void_p(st.cuda_stream)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB, twice the L2
+    # L2 eviction between timed steps: a 256 MB write (twice the L2), then a 256 MB read that
+    # writes those dirty lines back, so a timed step starts cold and inherits no write-back
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    clean = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    sink = torch.empty((), dtype=torch.float32, device=dev)
+
+    def evict(i):
+        flush.fill_(float(i))
+        torch.sum(clean, dim=0, out=sink)
 
     def step():
         rc = L.meke_b200_step(h, C.byref(margs), del2, sp)
@@ -877,7 +925,7 @@ def run_meke(args, rank, world, local_rank):
             RL.redi_b200_profile_begin()
         n0 = RL.redi_b200_launch_count(-1)
         for i in range(nsteps):
-            flush.fill_(float(i))  # evict the previous step's fields from L2
+            evict(i)
             ev[i][0].record(st)
             step()
             ev[i][1].record(st)

@@ -49,8 +49,10 @@ namespace {
 
 constexpr double kMassNeglect = 1.0e-30;  // meke/meke.F90:51 MASS_NEGLECT
 constexpr double kHVanished = 1.5e-4;     // meke/constants.F90:15 H_VANISHED
-constexpr int kThreads = 256;
-constexpr int kColumnBatch = 8;  // layers whose loads are in flight together
+constexpr int kThreadsA = 256;  // pass A block: one column per thread
+constexpr int kThreads = 128;   // pass B and Laplacian block: one cell per thread
+constexpr int kMinBlocksB = 8;  // pass B register cap: the whole benchmark grid in one wave
+constexpr int kColumnBatch = 8; // layers whose loads are in flight together
 
 thread_local std::string g_err;
 
@@ -106,8 +108,8 @@ __device__ __forceinline__ double harmonic_mass(double m1, double m2) {
 }
 
 // ---------------------------------------------------------------- pass A ----
-__global__ void __launch_bounds__(kThreads) k_meke_column(const MekeArgs a, const Plan p) {
-    const int t = blockIdx.x * kThreads + threadIdx.x;
+__global__ void __launch_bounds__(kThreadsA) k_meke_column(const MekeArgs a, const Plan p) {
+    const int t = blockIdx.x * kThreadsA + threadIdx.x;
     // pass B's blocks may be scheduled as soon as every block of this grid runs
     cudaTriggerProgrammaticLaunchCompletion();
     // meke_zero_2d of the staged SN faces (meke/meke.F90:82-83)
@@ -115,13 +117,22 @@ __global__ void __launch_bounds__(kThreads) k_meke_column(const MekeArgs a, cons
     if (t < p.nv) a.sn_v_ws[t] = 0.0;
     if (t >= p.nt) return;
 
-    // meke_mass (meke/meke.F90:355-388), have_rho: one in-order sum per column
+    // per-cell inputs first, so their latency hides under the column stream
+    const double kd = __ldg(a.ke_diss_ext + t);
+    const double area = __ldg(a.areaT + t);
+    const double ubbl2 = __ldg(a.u_bbl2 + t);
+    const double gm = a.gmcoeff >= 0.0 ? __ldg(a.gm_src + t) : 0.0;
+    const double e0 = a.meke[t];
+    const double kh_prev = p.kh_face ? a.kh_diff[t] : 0.0;
+
+    // meke_mass (meke/meke.F90:355-388), have_rho: one in-order sum per column.
     const size_t plane = (size_t)p.nt;
     const double* __restrict__ hcol = a.h_layer + t;
     const double* __restrict__ rcol = a.rho_layer + t;
+    const int nz = a.nz;
     double mass = 0.0, dsum = 0.0;
     int k = 0;
-    for (; k + kColumnBatch <= a.nz; k += kColumnBatch) {
+    for (; k + kColumnBatch <= nz; k += kColumnBatch) {
         double hv[kColumnBatch], rv[kColumnBatch];
 #pragma unroll
         for (int u = 0; u < kColumnBatch; ++u) {
@@ -134,7 +145,7 @@ __global__ void __launch_bounds__(kThreads) k_meke_column(const MekeArgs a, cons
             dsum = dsum + hv[u];
         }
     }
-    for (; k < a.nz; ++k) {
+    for (; k < nz; ++k) {
         const double hk = __ldg(hcol + (size_t)k * plane);
         const double rk = __ldg(rcol + (size_t)k * plane);
         mass = mass + rk * fmax(hk, kHVanished);
@@ -148,11 +159,9 @@ __global__ void __launch_bounds__(kThreads) k_meke_column(const MekeArgs a, cons
     // meke_zero_2d of rd (:81) and meke_stage_rd of ke_diss (:100)
     const double rd = 0.0;
     a.rd_ws[t] = rd;
-    const double kd = __ldg(a.ke_diss_ext + t);
     a.ke_diss_ws[t] = kd;
 
     // meke_length_scales (meke/meke.F90:420-505)
-    const double area = __ldg(a.areaT + t);
     const double lgrid = sqrt(fmax(area, 0.0));
     const double ldeform = lgrid * rd;
     double lfrict = 0.0;
@@ -160,16 +169,17 @@ __global__ void __launch_bounds__(kThreads) k_meke_column(const MekeArgs a, cons
     double bf2 = a.cd_scale * a.cd_scale;
     if (lfrict * a.cb > 0.0) {
         const double ratio = ldeform / lfrict;
-        bf2 = bf2 + 1.0 / pow(1.0 + a.cb * ratio, 0.8);
+        const double base = 1.0 + a.cb * ratio;  // exactly 1 here: rd is zero in this step
+        bf2 = bf2 + 1.0 / (base == 1.0 ? 1.0 : pow(base, 0.8));  // pow(+1, y) == 1 for every y
     }
     bf2 = fmax(bf2, a.min_gamma2);
     double tf2 = 1.0;
     if (lfrict * a.ct > 0.0) {
         const double ratio = ldeform / lfrict;
-        tf2 = 1.0 / pow(1.0 + a.ct * ratio, 0.25);
+        const double base = 1.0 + a.ct * ratio;
+        tf2 = 1.0 / (base == 1.0 ? 1.0 : pow(base, 0.25));
     }
     tf2 = fmax(tf2, a.min_gamma2);
-    const double e0 = a.meke[t];
     const double ueddy = sqrt(2.0 * fmax(0.0, tf2 * e0));
     double beta = 0.0;
     if (p.rhines) {
@@ -194,12 +204,12 @@ __global__ void __launch_bounds__(kThreads) k_meke_column(const MekeArgs a, cons
 
     // meke_source (meke/meke.F90:507-530) and the first drag half (:532-556)
     double s = a.bgsrc;
-    if (a.gmcoeff >= 0.0) s = s + a.gmcoeff * imass * __ldg(a.gm_src + t);
+    if (a.gmcoeff >= 0.0) s = s + a.gmcoeff * imass * gm;
     if (a.frcoeff >= 0.0) s = s - a.frcoeff * imass * kd;
     a.src[t] = s;
     const double e = e0 + p.sdt * s;
-    p.e1[t] = drag_half(e, imass, bf2, __ldg(a.u_bbl2 + t), a.cdrag, a.uscale, a.damping, p.sdt_damp);
-    if (p.kh_face) p.kh0[t] = a.kh_diff[t];
+    p.e1[t] = drag_half(e, imass, bf2, ubbl2, a.cdrag, a.uscale, a.damping, p.sdt_damp);
+    if (p.kh_face) p.kh0[t] = kh_prev;
 }
 
 // ------------------------------------------------- biharmonic Laplacian -----
@@ -221,28 +231,33 @@ __global__ void __launch_bounds__(kThreads) k_meke_del2(const MekeArgs a, const 
 }
 
 // ---------------------------------------------------------------- pass B ----
-// Laplacian flux through the face between cells tl and tr (tr = tl + 1 for a
-// u face, tl + nx for a v face) with face metrics fa * fb (meke/meke.F90:736-745).
-__device__ __forceinline__ double lap_flux(const MekeArgs& a, const Plan& p, int tl, int tr, double geo) {
+// Laplacian flux through a face from the values of its left / lower cell (l)
+// and right / upper cell (r) (meke/meke.F90:736-745).
+__device__ __forceinline__ double lap_face(const MekeArgs& a, const Plan& p, double geo, double ia_l, double ia_r,
+                                           double m_l, double m_r, double e_l, double e_r, double k_l, double k_r) {
     double kh = fmax(0.0, a.kh_bg);
-    if (p.kh_face) kh = kh + a.khmeke_fac * 0.5 * (p.kh0[tl] + p.kh0[tr]);
-    const double inv_max = 2.0 * p.sdt * (geo * fmax(__ldg(a.iareaT + tl), __ldg(a.iareaT + tr)));
+    if (p.kh_face) kh = kh + a.khmeke_fac * 0.5 * (k_l + k_r);
+    const double inv_max = 2.0 * p.sdt * (geo * fmax(ia_l, ia_r));
     if (kh * inv_max > 0.25) kh = 0.25 / inv_max;
-    const double hm = harmonic_mass(__ldg(a.mass_ws + tl), __ldg(a.mass_ws + tr));
-    return (kh * geo) * hm * (__ldg(p.e1 + tl) - __ldg(p.e1 + tr));
+    return (kh * geo) * harmonic_mass(m_l, m_r) * (e_l - e_r);
 }
 
 // Biharmonic flux of the Laplacian through the same face (meke/meke.F90:697-724).
-__device__ __forceinline__ double bih_flux(const MekeArgs& a, const Plan& p, int tl, int tr, double geo) {
-    const double g = geo * fmax(__ldg(a.iareaT + tl), __ldg(a.iareaT + tr));
+__device__ __forceinline__ double bih_face(const MekeArgs& a, const Plan& p, double geo, double ia_l, double ia_r,
+                                           double m_l, double m_r, double l_l, double l_r) {
+    const double g = geo * fmax(ia_l, ia_r);
     const double inv_max = 64.0 * p.sdt * (g * g);
     double k4 = a.k4;
     if (k4 * inv_max > 0.3) k4 = 0.3 / inv_max;
-    const double hm = harmonic_mass(__ldg(a.mass_ws + tl), __ldg(a.mass_ws + tr));
-    return (k4 * geo) * hm * (__ldg(p.lap + tr) - __ldg(p.lap + tl));
+    return (k4 * geo) * harmonic_mass(m_l, m_r) * (l_r - l_l);
 }
 
-__global__ void __launch_bounds__(kThreads) k_meke_lateral(const MekeArgs a, const Plan p) {
+// Every load of a thread is issued up front: neighbour indices are clamped into
+// the domain (an edge neighbour stands in as the cell itself, and that face's
+// flux is replaced by 0, the value meke_lateral gives edge faces), and the face
+// metrics of the edge faces exist (u faces have nx+1 columns, v faces ny+1
+// rows). Interior faces see exactly the reference's operands.
+__global__ void __launch_bounds__(kThreads, kMinBlocksB) k_meke_lateral(const MekeArgs a, const Plan p) {
     const int t = blockIdx.x * kThreads + threadIdx.x;
     if (p.pdl) cudaGridDependencySynchronize();
     if (t >= p.nt) return;
@@ -250,20 +265,41 @@ __global__ void __launch_bounds__(kThreads) k_meke_lateral(const MekeArgs a, con
     const int i = t % nx, j = t / nx;
     const int fu = t + j;  // u face west of cell t; the v face south of it is t
     const bool west = i > 0, east = i < nx - 1, south = j > 0, north = j < ny - 1;
-    const double geo_w = west ? __ldg(a.dy_cu + fu) * __ldg(a.idxCu + fu) : 0.0;
-    const double geo_e = east ? __ldg(a.dy_cu + fu + 1) * __ldg(a.idxCu + fu + 1) : 0.0;
-    const double geo_s = south ? __ldg(a.dx_cv + t) * __ldg(a.idyCv + t) : 0.0;
-    const double geo_n = north ? __ldg(a.dx_cv + t + nx) * __ldg(a.idyCv + t + nx) : 0.0;
+    const int tw = west ? t - 1 : t, te = east ? t + 1 : t, ts = south ? t - nx : t, tn = north ? t + nx : t;
+
+    const double geo_w = __ldg(a.dy_cu + fu) * __ldg(a.idxCu + fu);
+    const double geo_e = __ldg(a.dy_cu + fu + 1) * __ldg(a.idxCu + fu + 1);
+    const double geo_s = __ldg(a.dx_cv + t) * __ldg(a.idyCv + t);
+    const double geo_n = __ldg(a.dx_cv + t + nx) * __ldg(a.idyCv + t + nx);
+    const double* __restrict__ iar = a.iareaT;
+    const double* __restrict__ mws = a.mass_ws;
+    const double* __restrict__ e1 = p.e1;
+    const double ia_c = __ldg(iar + t), ia_w = __ldg(iar + tw), ia_e = __ldg(iar + te), ia_s = __ldg(iar + ts),
+                 ia_n = __ldg(iar + tn);
+    const double m_c = __ldg(mws + t), m_w = __ldg(mws + tw), m_e = __ldg(mws + te), m_s = __ldg(mws + ts),
+                 m_n = __ldg(mws + tn);
     const double imass = __ldg(a.i_mass + t);
-    const double ia = __ldg(a.iareaT + t);
-    double e = __ldg(p.e1 + t);
+    const double bf2 = __ldg(a.bottom_fac2 + t);
+    const double ubbl2 = __ldg(a.u_bbl2 + t);
+    const double tf2 = __ldg(a.barotr_fac2 + t);
+    const double lmix = __ldg(a.le + t);
+    double e = __ldg(e1 + t);
 
     if (p.kh_flux) {
         // meke_lateral, Laplacian block (meke/meke.F90:732-746)
-        const double fw = west ? lap_flux(a, p, t - 1, t, geo_w) : 0.0;
-        const double fe = east ? lap_flux(a, p, t, t + 1, geo_e) : 0.0;
-        const double fs = south ? lap_flux(a, p, t - nx, t, geo_s) : 0.0;
-        const double fn = north ? lap_flux(a, p, t, t + nx, geo_n) : 0.0;
+        const double e_w = __ldg(e1 + tw), e_e = __ldg(e1 + te), e_s = __ldg(e1 + ts), e_n = __ldg(e1 + tn);
+        double k_c = 0.0, k_w = 0.0, k_e = 0.0, k_s = 0.0, k_n = 0.0;
+        if (p.kh_face) {
+            k_c = __ldg(p.kh0 + t);
+            k_w = __ldg(p.kh0 + tw);
+            k_e = __ldg(p.kh0 + te);
+            k_s = __ldg(p.kh0 + ts);
+            k_n = __ldg(p.kh0 + tn);
+        }
+        const double fw = west ? lap_face(a, p, geo_w, ia_w, ia_c, m_w, m_c, e_w, e, k_w, k_c) : 0.0;
+        const double fe = east ? lap_face(a, p, geo_e, ia_c, ia_e, m_c, m_e, e, e_e, k_c, k_e) : 0.0;
+        const double fs = south ? lap_face(a, p, geo_s, ia_s, ia_c, m_s, m_c, e_s, e, k_s, k_c) : 0.0;
+        const double fn = north ? lap_face(a, p, geo_n, ia_c, ia_n, m_c, m_n, e, e_n, k_c, k_n) : 0.0;
         if (a.uflux) {
             a.uflux[fu] = fw;
             if (!east) a.uflux[fu + 1] = 0.0;
@@ -272,14 +308,17 @@ __global__ void __launch_bounds__(kThreads) k_meke_lateral(const MekeArgs a, con
             a.vflux[t] = fs;
             if (!north) a.vflux[t + nx] = 0.0;
         }
-        const double mke = p.sdt * (ia * imass) * ((fw - fe) + (fs - fn));
+        const double mke = p.sdt * (ia_c * imass) * ((fw - fe) + (fs - fn));
         e = e + mke;
     }
     if (p.biharmonic) {
-        const double gw = west ? bih_flux(a, p, t - 1, t, geo_w) : 0.0;
-        const double ge = east ? bih_flux(a, p, t, t + 1, geo_e) : 0.0;
-        const double gs = south ? bih_flux(a, p, t - nx, t, geo_s) : 0.0;
-        const double gn = north ? bih_flux(a, p, t, t + nx, geo_n) : 0.0;
+        const double* __restrict__ lap = p.lap;
+        const double l_c = __ldg(lap + t), l_w = __ldg(lap + tw), l_e = __ldg(lap + te), l_s = __ldg(lap + ts),
+                     l_n = __ldg(lap + tn);
+        const double gw = west ? bih_face(a, p, geo_w, ia_w, ia_c, m_w, m_c, l_w, l_c) : 0.0;
+        const double ge = east ? bih_face(a, p, geo_e, ia_c, ia_e, m_c, m_e, l_c, l_e) : 0.0;
+        const double gs = south ? bih_face(a, p, geo_s, ia_s, ia_c, m_s, m_c, l_s, l_c) : 0.0;
+        const double gn = north ? bih_face(a, p, geo_n, ia_c, ia_n, m_c, m_n, l_c, l_n) : 0.0;
         if (!p.kh_flux) {  // the biharmonic fluxes are then the last ones meke_lateral stores
             if (a.uflux) {
                 a.uflux[fu] = gw;
@@ -290,19 +329,17 @@ __global__ void __launch_bounds__(kThreads) k_meke_lateral(const MekeArgs a, con
                 if (!north) a.vflux[t + nx] = 0.0;
             }
         }
-        const double mke4 = p.sdt * (ia * imass) * ((gw - ge) + (gs - gn));
+        const double mke4 = p.sdt * (ia_c * imass) * ((gw - ge) + (gs - gn));
         p.del2[t] = mke4;
         e = e + mke4;
     }
-    const double bf2 = __ldg(a.bottom_fac2 + t);
-    if (p.drag2) e = drag_half(e, imass, bf2, __ldg(a.u_bbl2 + t), a.cdrag, a.uscale, a.damping, p.sdt_damp);
+    if (p.drag2) e = drag_half(e, imass, bf2, ubbl2, a.cdrag, a.uscale, a.damping, p.sdt_damp);
     a.meke[t] = e;
 
     // meke_kh_closure and meke_ku_closure (meke/meke.F90:575-622)
-    const double lmix = __ldg(a.le + t);
     double kh = 0.0;
     if (a.khcoeff > 0.0) {
-        const double ueddy = sqrt(2.0 * fmax(0.0, __ldg(a.barotr_fac2 + t) * e));
+        const double ueddy = sqrt(2.0 * fmax(0.0, tf2 * e));
         kh = a.khcoeff * ueddy * lmix;
     }
     a.kh_diff[t] = kh;
@@ -367,7 +404,7 @@ int blocks(int n) { return (n + kThreads - 1) / kThreads; }
 int launch_step(const MekeArgs& a, Plan p, cudaStream_t st, bool pdl, bool instrument) {
     const int na = p.nu > p.nv ? p.nu : p.nv;  // >= nt
     if (instrument) redi::launch_begin(redi::K_MEKE_COLUMN, st);
-    k_meke_column<<<blocks(na), kThreads, 0, st>>>(a, p);
+    k_meke_column<<<(na + kThreadsA - 1) / kThreadsA, kThreadsA, 0, st>>>(a, p);
     if (instrument) redi::launch_end(redi::K_MEKE_COLUMN, st);
     if (p.biharmonic) {
         if (instrument) redi::launch_begin(redi::K_MEKE_DEL2, st);
@@ -525,7 +562,8 @@ void meke_cuda_launch(const MekeArgs* ap, int mode) {
             g_graph.reset();
         cudaError_t e = cudaSuccess;
         if (!g_graph.valid) {
-            e = cudaStreamCreateWithFlags(&g_graph.stream, cudaStreamNonBlocking);
+            // a blocking stream, as the reference's: ordered with the legacy default stream
+            e = cudaStreamCreate(&g_graph.stream);
             cudaGraph_t g = nullptr;
             if (e == cudaSuccess) e = cudaStreamBeginCapture(g_graph.stream, cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {

@@ -52,7 +52,9 @@ def main():
         L.meke_opt_launch.restype = None
         L.meke_cuda_graph_reset.restype = None
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    out = {"grid_arrays": [p.nx, p.ny, p.nz], "reps": args.reps, "l2": "flushed before every call"}
+    clean = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    sink = torch.empty((), dtype=torch.float32, device="cuda")
+    out = {"grid_arrays": [p.nx, p.ny, p.nz], "reps": args.reps, "l2": "evicted (write + read) before every call"}
 
     def timed(fn):
         for _ in range(3):
@@ -60,7 +62,8 @@ def main():
         torch.cuda.synchronize()
         ts = []
         for i in range(args.reps):
-            flush.fill_(float(i))
+            flush.fill_(float(i))  # evict the L2: a 256 MB write, then a 256 MB read
+            torch.sum(clean, dim=0, out=sink)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             fn()
