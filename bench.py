@@ -53,7 +53,7 @@ METRIC = "Redi tracer-cell updates/s, HBM GB/s; mixed+batched vs FP64 plain, 1 B
 UNIT = "tracer-cell updates/s"
 KERNEL_NAMES = ["k_column_state", "k_neutral_sweep", "k_tracer_recon", "k_cell_gather", "k_face_flux",
                 "k_mixed_recon", "k_mixed_flux", "k_mixed_sweep", "k_domain_persistent", "aux",
-                "k_meke_column", "k_meke_del2", "k_meke_lateral"]
+                "k_meke_column", "k_meke_del2", "k_meke_lateral", "k_ale_columns", "k_ale_faces"]
 NKERN = len(KERNEL_NAMES)
 FALLBACK_HBM_GBS = 6650.0
 
@@ -1022,6 +1022,226 @@ def run_meke(args, rank, world, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# ALE remap step (ale_remap_step): zstar target, PPM remap of T, S and the face velocities
+# ---------------------------------------------------------------------------
+ALE_METRIC = "ALE remap column-steps/s (ale_remap_step, zstar, PPM, T+S, face velocities), 1 B200"
+ALE_UNIT = "column-steps/s"
+
+
+def _ale_problem(config: str):
+    from more_benchmarks_dc_ocean_b200 import ale_inputs as AI
+
+    if config == "ale":  # the reference's benchmark: 473 x 297 points, 3 ghosts, 30 layers, h-drift 25 %
+        return AI.reference_ic()
+    return AI.reference_ic(1440, 1080, 75, nghost=2)  # ale_c1: the Redi config-1 grid
+
+
+def ale_bytes(nx: int, ny: int, nz: int):
+    """Algorithmic bytes of the ALE kernels per step (column tiles, face tiles), PPM, T and S.
+
+    columns: read h, write h_old and target_h, read + write T, S, the heat, salt and mass budgets,
+    write h_layer; faces: read h_old and target_h once, read + write u and v (2-D fields are
+    negligible and not counted)."""
+    n3, nu3, nv3 = nx * ny * nz, (nx + 1) * ny * nz, nx * (ny + 1) * nz
+    return 8.0 * 14 * n3, 8.0 * (2 * n3 + 2 * nu3 + 2 * nv3)
+
+
+def ale_cpu_sample(p, target_s: float, nsteps: int = 0, warmup: int = 0):
+    from oracle import ale_oracle as AO
+
+    threads = len(os.sched_getaffinity(0))
+    q = p.copy()
+    t0 = time.perf_counter()
+    AO.step(q, 1)
+    probe = max(time.perf_counter() - t0, 1e-4)
+    n = nsteps or int(max(2, min(100, target_s / probe)))
+    times = []
+    for s in range(warmup + n):
+        q = p.copy()  # from the pristine state, as the timed GPU steps
+        t0 = time.perf_counter()
+        AO.step(q, 1)
+        if s >= warmup:
+            times.append(time.perf_counter() - t0)
+    t = min(times)
+    return p.nx * p.ny / t, {"cores": threads, "t_step_s": t, "steps": n,
+                             "sample": f"{p.nx}x{p.ny}x{p.nz} ({p.name}), whole domain from the pristine state, "
+                                       f"min of {n} step(s)"}
+
+
+def _ale_config_block(p, world):
+    return {"workload": f"ALE remap {p.nx}x{p.ny}x{p.nz} (arrays incl. ghosts), zstar target, PPM, T+S with "
+                        f"budgets, u/v face velocities, h-drift 25 %" + (f", {world} replicas" if world > 1 else ""),
+            "grid": [p.nx, p.ny, p.nz],
+            "l2": "state restored from the pristine copy, then L2 evicted (256 MB write + 256 MB read), before "
+                  "every timed step",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"}
+
+
+def run_ale_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    p = _ale_problem(args.config)
+    per = max(1.0, 120.0 / max(1, args.steps + args.warmup))
+    val, info = ale_cpu_sample(p, per, nsteps=args.steps, warmup=args.warmup)
+    print(json.dumps({
+        "impl": "reference", "metric": ALE_METRIC, "value": val, "unit": ALE_UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": info["t_step_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": _ale_config_block(p, world),
+        "cpu_baseline": {"value": val, "unit": ALE_UNIT, "cores": info["cores"], "kind": "port",
+                         "sample": info["sample"]},
+        "e2e": {"value": val, "unit": ALE_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU path (ale_remap_step restated in C++, OpenMP over all host cores); the Fortran "
+                "build itself needs a Fortran compiler, absent on this image"}), flush=True)
+    return 0
+
+
+def run_ale(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+
+    from more_benchmarks_dc_ocean_b200 import ale_remap as A
+    from more_benchmarks_dc_ocean_b200 import ocean_redi as R
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:  # independent replicas: the step has no exchange of its own
+        import torch.distributed as dist  # noqa: F811
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    p = _ale_problem(args.config)
+    d = A.to_device(p, dev)
+    prist = {k: d[k].clone() for k in ("h_layer", "u", "v", "mass_budget", "heat_budget", "salt_budget", "bt_eta")}
+    prist_tr = [t.clone() for t in d["tracers"]]
+    RL = R.lib()
+    RL.redi_b200_launch_count.restype = C.c_ulonglong
+    RL.redi_b200_launch_count.argtypes = [C.c_int]
+    st = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    clean = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    sink = torch.empty((), dtype=torch.float32, device=dev)
+
+    def restore():
+        for k, v in prist.items():
+            d[k].copy_(v)
+        for a, b in zip(d["tracers"], prist_tr):
+            a.copy_(b)
+
+    def evict(i):
+        flush.fill_(float(i))
+        torch.sum(clean, dim=0, out=sink)
+
+    def step():
+        A.step_problem(p, d, 1, st)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        restore()
+        step()
+    torch.cuda.synchronize()
+
+    def timed(nsteps, profile=False):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+        if profile:
+            RL.redi_b200_profile_begin()
+        n0 = RL.redi_b200_launch_count(-1)
+        for i in range(nsteps):
+            restore()
+            evict(i)
+            ev[i][0].record(st)
+            step()
+            ev[i][1].record(st)
+        torch.cuda.synchronize()
+        n1 = RL.redi_b200_launch_count(-1)
+        kt = (C.c_double * NKERN)()
+        kc = (C.c_ulonglong * NKERN)()
+        if profile:
+            RL.redi_b200_profile_end(kt, kc, NKERN)
+        return sum(a.elapsed_time(b) for a, b in ev) / nsteps, int(n1 - n0), kt, kc
+
+    clocks = ClockSampler(_uuid(local_rank))
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ms, launches, _, _ = timed(args.steps)
+    barrier()
+    clk = clocks.stop()
+    ms_all = _max_over_ranks(ms, dist, dev)
+    value = p.nx * p.ny * world / (ms_all * 1e-3)
+    _, _, kt, kc = timed(args.steps, profile=True)
+    kern = {KERNEL_NAMES[k]: {"ms_total": kt[k], "launches": int(kc[k]), "ms_per_launch": kt[k] / kc[k]}
+            for k in range(NKERN) if kc[k]}
+    b_col, b_fc = ale_bytes(p.nx, p.ny, p.nz)
+    kb = {13: b_col, 14: b_fc}
+    top = max((k for k in kb if kc[k]), key=lambda k: kt[k])
+    peak, peak_kind = _peaks()
+    achieved = kb[top] / (kt[top] / kc[top] * 1e-3) / 1e9
+    traffic = _ncu_traffic_tag("ale" if args.config == "ale" else "ale_c1").get(KERNEL_NAMES[top])
+    total_b = b_col + b_fc
+
+    e2e = None
+    if not args.no_e2e:
+        keys = ("h_layer", "u", "v", "mass_budget", "heat_budget", "salt_budget", "bt_eta")
+        host = {k: prist[k].cpu().pin_memory() for k in keys}
+        host_tr = [t.cpu().pin_memory() for t in prist_tr]
+
+        def e2e_step():
+            for k in keys:
+                d[k].copy_(host[k], non_blocking=True)
+            for a, b in zip(d["tracers"], host_tr):
+                a.copy_(b, non_blocking=True)
+            step()
+            for k in keys:
+                host[k].copy_(d[k], non_blocking=True)
+            for a, b in zip(d["tracers"], host_tr):
+                b.copy_(a, non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        for _ in range(args.steps):
+            e2e_step()
+        b.record(st)
+        torch.cuda.synchronize()
+        ems = _max_over_ranks(a.elapsed_time(b) / args.steps, dist, dev)
+        nbytes = int(sum(host[k].numel() * 8 for k in keys) + sum(t.numel() * 8 for t in host_tr))
+        e2e = {"value": p.nx * p.ny * world / (ems * 1e-3), "unit": ALE_UNIT, "ms_per_step": ems,
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "host_memory": "pinned",
+               "path": "ale_b200_remap_step with the model state copied up and back every step"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, info = ale_cpu_sample(p, args.cpu_seconds)
+        cpu = {"value": v, "unit": ALE_UNIT, "cores": info["cores"], "kind": "port", "sample": info["sample"]}
+
+    if rank == 0:
+        print(json.dumps({
+            "metric": ALE_METRIC, "value": value, "unit": ALE_UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_all, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": _ale_config_block(p, world),
+            "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[top], "achieved": achieved, "peak": peak,
+                         "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": kb[top]},
+            "step_roofline": {"algorithmic_bytes_per_step": total_b,
+                              "achieved_gbs": total_b / (ms_all * 1e-3) / 1e9,
+                              "frac": total_b / (ms_all * 1e-3) / 1e9 / peak},
+            "kernels": kern, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches}), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1029,7 +1249,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="config1",
-                    choices=["config0", "config1", "config3", "config4", "meke", "meke_c1"])
+                    choices=["config0", "config1", "config3", "config4", "meke", "meke_c1", "ale", "ale_c1"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: a generated domain of that size instead of --config")
     ap.add_argument("--no-e2e", action="store_true")
@@ -1044,9 +1264,13 @@ def main():
     if args.impl == "reference":
         if args.config.startswith("meke"):
             return run_meke_reference(args, rank, world)
+        if args.config.startswith("ale"):
+            return run_ale_reference(args, rank, world)
         return run_reference(args, rank, world)
     if args.config.startswith("meke"):
         return run_meke(args, rank, world, local_rank)
+    if args.config.startswith("ale"):
+        return run_ale(args, rank, world, local_rank)
     if args.config == "config4":
         return run_domains(args, rank, world, local_rank)
     return run_b200(args, rank, world, local_rank)

@@ -186,7 +186,8 @@ REDI_B200_API int redi_b200_version(void);
  * 0 column_state, 1 neutral_sweep, 2 tracer_recon, 3 cell_gather (the per-cell
  * update), 4 face_flux, 5 mixed_recon, 6 mixed_flux, 7 mixed_sweep,
  * 8 domain_persistent, 9 auxiliary, and the MEKE step's (meke_b200.h) 10 pass A,
- * 11 biharmonic Laplacian, 12 pass B; redi_b200_kernel_count() is their number.
+ * 11 biharmonic Laplacian, 12 pass B, and the ALE remap step's (ale_b200.h) 13 column
+ * tiles, 14 face tiles; redi_b200_kernel_count() is their number.
  * redi_b200_launch_count(k) counts launches of kernel k since load (k < 0:
  * all). Between profile_begin and profile_end every launch is bracketed by a
  * CUDA event pair on its own stream; profile_end waits for them and returns,

@@ -1,6 +1,6 @@
 """Build the sm_100a shared library (libredi_b200.so) in-tree with nvcc.
 
-The kernels (redi_plain.cu, redi_domains.cu, meke.cu) are compiled with FMA contraction off so their
+The kernels (redi_plain.cu, redi_domains.cu, meke.cu, ale.cu) are compiled with FMA contraction off so their
 arithmetic is the reference's IEEE sequence; everything is compiled for
 sm_100a only (`-gencode arch=compute_100a,code=sm_100a`).
 """
@@ -28,6 +28,7 @@ SOURCES = [
     ("redi_noalloc.cu", []),
     ("redi_domains.cu", ["-fmad=false"]),
     ("meke.cu", ["-fmad=false"]),
+    ("ale.cu", ["-fmad=false"]),
 ]
 
 
@@ -50,7 +51,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     nvcc = _nvcc()
     os.makedirs(BUILD_DIR, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    headers += [os.path.join(INCLUDE, "redi_b200.h"), os.path.join(INCLUDE, "meke_b200.h")]
+    headers += [os.path.join(INCLUDE, h) for h in ("redi_b200.h", "meke_b200.h", "ale_b200.h")]
     objs = []
     for src, flags in SOURCES:
         path = os.path.join(CSRC, src)

@@ -177,7 +177,9 @@ enum KernelId : int {
     K_MEKE_COLUMN = 10,   // MEKE pass A
     K_MEKE_DEL2 = 11,     // MEKE biharmonic Laplacian
     K_MEKE_LATERAL = 12,  // MEKE pass B
-    K_NUM = 13
+    K_ALE_COLUMNS = 13,   // ALE remap: targets, snapshot, tracers and the commit
+    K_ALE_FACES = 14,     // ALE remap: face velocities
+    K_NUM = 15
 };
 
 // Sets the message redi_b200_last_error() returns on the calling thread.

@@ -8,10 +8,13 @@
 #                        redi/opt_kernel.cu (`redi_opt_launch`)
 #   libmeke_refcuda.so   meke/meke_kernel.cu (`meke_cuda_launch`) and
 #                        meke/opt_kernel.cu (`meke_opt_launch`)
+#   libale_refcuda.so    ale_remap/ale_kernel.cu (`ale_remap_cuda`) and
+#                        ale_remap/opt_kernel.cu (`ale_remap_opt`)
 #
 # Built as the reference's Makefiles build them (redi/Makefile:57-63: -O3,
 # -I../common, -DMODEL_NZ_STACK_MAX=128 -DWITH_CUDA; meke/Makefile CUFLAGS:
-# -O3, -I../common -I.) except for two flags: the target is sm_100a, and FMA
+# -O3, -I../common -I.; ale_remap/Makefile CUFLAGS: -O3, -I../common,
+# -DMODEL_NZ_STACK_MAX=128) except for two flags: the target is sm_100a, and FMA
 # contraction is off (-fmad=false) so the result is the IEEE sequence of the
 # source, comparable bit for bit. The *_native.so twins keep the reference's
 # own flags (FMA contraction on) and are used only for timing.
@@ -57,4 +60,7 @@ build_pair() {
 build_pair redi "$REF/redi" -DMODEL_NZ_STACK_MAX=128 -DWITH_CUDA -- redi_kernel.cu opt_kernel.cu
 if [[ -f "$REF/meke/meke_kernel.cu" ]]; then
   build_pair meke "$REF/meke" -- meke_kernel.cu opt_kernel.cu
+fi
+if [[ -f "$REF/ale_remap/ale_kernel.cu" ]]; then
+  build_pair ale "$REF/ale_remap" -DMODEL_NZ_STACK_MAX=128 -- ale_kernel.cu opt_kernel.cu
 fi
