@@ -43,7 +43,7 @@ namespace {
 
 constexpr double kHFloor = 1.5e-4;  // ale_remap/ale_remap.F90:70 H_FLOOR
 constexpr int kNzMax = ALE_B200_NZ_MAX;
-constexpr int kThreads = 256;
+constexpr int kThreads = 256;  // with a 64-register cap: four blocks per SM
 constexpr int kMaxTracers = 8;  // tracers remapped by one launch
 constexpr int kPCM = 1, kPLM = 2, kPPM = 3;
 
@@ -51,7 +51,7 @@ thread_local std::string g_err;
 
 struct Dims {
     int nx, ny, nz, conserve_ke;
-    long long n2;  // cells per layer
+    int n2;  // cells per layer (every offset of a step fits in 32 bits: checked on the host)
 };
 
 struct TracerSet {
@@ -60,11 +60,11 @@ struct TracerSet {
     double* budget[kMaxTracers];
 };
 
-// A column of a tile in shared memory: element k at p[k * stride].
+// A column of a tile in shared memory: element k at p[k * S].
+template <int S>
 struct Col {
     const double* p;
-    int stride;
-    __device__ __forceinline__ double operator[](int k) const { return p[k * stride]; }
+    __device__ __forceinline__ double operator[](int k) const { return p[k * S]; }
 };
 
 // Tile width (columns) for a column capacity: the staged arrays stay within the shared memory of a block.
@@ -230,8 +230,9 @@ __device__ void serial_column(int nz, const A& dz_old, const A& z_old, const A& 
 }
 
 // rescale_anomaly_ke (ale_remap/ale_remap.F90:684-724) on one column of a tile
-__device__ void rescale_anomaly_ke(int nz, const Col& h_old, const Col& h_new, const Col& u_old, double* u_new,
-                                   int stride) {
+template <int stride>
+__device__ void rescale_anomaly_ke(int nz, const Col<stride>& h_old, const Col<stride>& h_new,
+                                   const Col<stride>& u_old, double* u_new) {
     double h_old_sum = 0.0, h_new_sum = 0.0, mom_old = 0.0, mom_new = 0.0;
     for (int k = 0; k < nz; ++k) {
         h_old_sum = h_old_sum + h_old[k];
@@ -282,7 +283,7 @@ __device__ __forceinline__ void tile_depths(int nz, int ncol, const double* dzo,
 // Tile of cell columns. pre: compute the snapshot and the targets from h_layer
 // (the first launch of a step); otherwise read them back. commit: the last launch.
 template <int METHOD, int CAP>
-__global__ void __launch_bounds__(kThreads) k_ale_columns(const Dims d, const TracerSet ts, int pre, int commit,
+__global__ void __launch_bounds__(kThreads, 4) k_ale_columns(const Dims d, const TracerSet ts, int pre, int commit,
                                                           double* h_layer, double* bt_eta,
                                                           const double* __restrict__ bt_H_ref,
                                                           const double* __restrict__ dsig, double* total_h,
@@ -298,8 +299,8 @@ __global__ void __launch_bounds__(kThreads) k_ale_columns(const Dims d, const Tr
     __shared__ int serial[W];
     __shared__ double ct[W];  // column total h_ref + eta of the zstar target
     const int nz = d.nz;
-    const long long n2 = d.n2;
-    const long long t0 = (long long)blockIdx.x * W;
+    const int n2 = d.n2;
+    const int t0 = blockIdx.x * W;
     const int ncol = (int)(n2 - t0 < W ? n2 - t0 : W);
     const int ne = nz * W;
 
@@ -352,18 +353,18 @@ __global__ void __launch_bounds__(kThreads) k_ale_columns(const Dims d, const Tr
         for (int e = threadIdx.x; e < ne; e += kThreads) {
             const int k = e / W, c = e - k * W;
             if (c >= ncol || serial[c]) continue;
-            const double cn = new_layer<METHOD>(nz, Col{dzo + c, W}, Col{zo + c, W}, Col{dzn + c, W},
-                                                Col{zn + c, W}, Col{q + c, W}, k);
-            const long long o = t0 + c + n2 * k;
+            const double cn = new_layer<METHOD>(nz, Col<W>{dzo + c}, Col<W>{zo + c}, Col<W>{dzn + c},
+                                                Col<W>{zn + c}, Col<W>{q + c}, k);
+            const int o = t0 + c + n2 * k;
             const double hTr_new = cn * dzn[e];
             if (budget) budget[o] = budget[o] + (hTr_new - hTr[o]);
             hTr[o] = hTr_new;
         }
         if (threadIdx.x < ncol && serial[threadIdx.x]) {
             const int c = threadIdx.x;
-            serial_column<METHOD>(nz, Col{dzo + c, W}, Col{zo + c, W}, Col{dzn + c, W}, Col{q + c, W},
+            serial_column<METHOD>(nz, Col<W>{dzo + c}, Col<W>{zo + c}, Col<W>{dzn + c}, Col<W>{q + c},
                                   [&](int k, double cn) {
-                                      const long long o = t0 + c + n2 * k;
+                                      const int o = t0 + c + n2 * k;
                                       const double hTr_new = cn * dzn[k * W + c];
                                       if (budget) budget[o] = budget[o] + (hTr_new - hTr[o]);
                                       hTr[o] = hTr_new;
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(kThreads) k_ale_columns(const Dims d, const Tr
         for (int e = threadIdx.x; e < ne; e += kThreads) {  // L9
             const int k = e / W, c = e - k * W;
             if (c >= ncol) continue;
-            const long long o = t0 + c + n2 * k;
+            const int o = t0 + c + n2 * k;
             mass_budget[o] = mass_budget[o] + (dzn[e] - dzo[e]);
             h_layer[o] = dzn[e];
         }
@@ -391,7 +392,7 @@ __global__ void __launch_bounds__(kThreads) k_ale_columns(const Dims d, const Tr
 
 // Tile of u faces (blocks [0, nbu)) or v faces (the rest).
 template <int METHOD, int CAP>
-__global__ void __launch_bounds__(kThreads) k_ale_faces(const Dims d, int nbu, const double* __restrict__ h_old,
+__global__ void __launch_bounds__(kThreads, 4) k_ale_faces(const Dims d, int nbu, const double* __restrict__ h_old,
                                                         const double* __restrict__ target_h, double* u, double* v) {
     constexpr int W = Tile<CAP>::W;
     extern __shared__ double sm[];
@@ -402,36 +403,36 @@ __global__ void __launch_bounds__(kThreads) k_ale_faces(const Dims d, int nbu, c
     double* q = zn + (CAP + 1) * W;
     double* qn = q + CAP * W;  // new values, when the KE rescale needs the whole column
     __shared__ int serial[W];
-    __shared__ long long cell_l[W], cell_r[W];
+    __shared__ int cell_l[W], cell_r[W];
     __shared__ int edge[W];
     const int nx = d.nx, ny = d.ny, nz = d.nz;
-    const long long n2 = d.n2;
+    const int n2 = d.n2;
     const bool xface = (int)blockIdx.x < nbu;
-    const long long nf = xface ? (long long)(nx + 1) * ny : (long long)nx * (ny + 1);
-    const long long f0 = (long long)(xface ? blockIdx.x : blockIdx.x - nbu) * W;
+    const int nf = xface ? (nx + 1) * ny : nx * (ny + 1);
+    const int f0 = (xface ? (int)blockIdx.x : (int)blockIdx.x - nbu) * W;
     const int ncol = (int)(nf - f0 < W ? nf - f0 : W);
     double* field = xface ? u : v;
     const int ne = nz * W;
 
     if (threadIdx.x < ncol) {
-        const long long f = f0 + threadIdx.x;
+        const int f = f0 + threadIdx.x;
         if (xface) {  // remap_x_face_velocity
             const int I = (int)(f % (nx + 1)), j = (int)(f / (nx + 1));
             edge[threadIdx.x] = I == 0 || I == nx;
-            cell_l[threadIdx.x] = (long long)(I == 0 ? 0 : I - 1) + (long long)nx * j;
-            cell_r[threadIdx.x] = (long long)(I == nx ? nx - 1 : I) + (long long)nx * j;
+            cell_l[threadIdx.x] = (I == 0 ? 0 : I - 1) + nx * j;
+            cell_r[threadIdx.x] = (I == nx ? nx - 1 : I) + nx * j;
         } else {  // remap_y_face_velocity
             const int i = (int)(f % nx), J = (int)(f / nx);
             edge[threadIdx.x] = J == 0 || J == ny;
-            cell_l[threadIdx.x] = (long long)i + (long long)nx * (J == 0 ? 0 : J - 1);
-            cell_r[threadIdx.x] = (long long)i + (long long)nx * (J == ny ? ny - 1 : J);
+            cell_l[threadIdx.x] = i + nx * (J == 0 ? 0 : J - 1);
+            cell_r[threadIdx.x] = i + nx * (J == ny ? ny - 1 : J);
         }
     }
     __syncthreads();
     for (int e = threadIdx.x; e < ne; e += kThreads) {
         const int k = e / W, c = e - k * W;
         if (c >= ncol) continue;
-        const long long l = cell_l[c] + n2 * k, r = cell_r[c] + n2 * k;
+        const int l = cell_l[c] + n2 * k, r = cell_r[c] + n2 * k;
         if (edge[c]) {
             dzo[e] = __ldg(h_old + l);
             dzn[e] = __ldg(target_h + l);
@@ -448,8 +449,8 @@ __global__ void __launch_bounds__(kThreads) k_ale_faces(const Dims d, int nbu, c
     for (int e = threadIdx.x; e < ne; e += kThreads) {
         const int k = e / W, c = e - k * W;
         if (c >= ncol || serial[c]) continue;
-        const double val = new_layer<METHOD>(nz, Col{dzo + c, W}, Col{zo + c, W}, Col{dzn + c, W}, Col{zn + c, W},
-                                             Col{q + c, W}, k);
+        const double val = new_layer<METHOD>(nz, Col<W>{dzo + c}, Col<W>{zo + c}, Col<W>{dzn + c}, Col<W>{zn + c},
+                                             Col<W>{q + c}, k);
         if (ke)
             qn[e] = val;
         else
@@ -457,7 +458,7 @@ __global__ void __launch_bounds__(kThreads) k_ale_faces(const Dims d, int nbu, c
     }
     if (threadIdx.x < ncol && serial[threadIdx.x]) {
         const int c = threadIdx.x;
-        serial_column<METHOD>(nz, Col{dzo + c, W}, Col{zo + c, W}, Col{dzn + c, W}, Col{q + c, W},
+        serial_column<METHOD>(nz, Col<W>{dzo + c}, Col<W>{zo + c}, Col<W>{dzn + c}, Col<W>{q + c},
                               [&](int k, double val) {
                                   if (ke)
                                       qn[k * W + c] = val;
@@ -469,7 +470,7 @@ __global__ void __launch_bounds__(kThreads) k_ale_faces(const Dims d, int nbu, c
     __syncthreads();
     if (threadIdx.x < ncol) {
         const int c = threadIdx.x;
-        rescale_anomaly_ke(nz, Col{dzo + c, W}, Col{dzn + c, W}, Col{q + c, W}, qn + c, W);
+        rescale_anomaly_ke<W>(nz, Col<W>{dzo + c}, Col<W>{dzn + c}, Col<W>{q + c}, qn + c);
     }
     __syncthreads();
     for (int e = threadIdx.x; e < ne; e += kThreads) {
@@ -512,7 +513,7 @@ int launch(const ale_b200_step_args& a, cudaStream_t st) {
     constexpr int W = Tile<CAP>::W;
     cudaError_t e = allow_smem<METHOD, CAP>();
     if (e != cudaSuccess) return fail(ALE_B200_E_CUDA, std::string("ale: shared memory: ") + cudaGetErrorString(e));
-    const Dims d{a.nx, a.ny, a.nz, a.conserve_ke ? 1 : 0, (long long)a.nx * a.ny};
+    const Dims d{a.nx, a.ny, a.nz, a.conserve_ke ? 1 : 0, a.nx * a.ny};
     std::vector<TracerSet> sets;
     TracerSet cur{};
     for (int n = 0; n < a.ntracers; ++n) {
@@ -557,8 +558,8 @@ int run(const ale_b200_step_args* a, cudaStream_t st) {
     if (!a) return fail(ALE_B200_E_ARG, "ale: NULL argument block");
     if (a->nx < 1 || a->ny < 1 || a->nz < 1) return fail(ALE_B200_E_ARG, "ale: nx, ny, nz must be >= 1");
     if (a->nz > kNzMax) return fail(ALE_B200_E_ARG, "ale: nz exceeds ALE_B200_NZ_MAX (the reference's NZ_STACK_MAX)");
-    if ((long long)(a->nx + 1) * (a->ny + 1) > (long long)INT_MAX)
-        return fail(ALE_B200_E_ARG, "ale: domain too large");
+    if ((long long)(a->nx + 1) * (a->ny + 1) * a->nz > (long long)INT_MAX - 1024)
+        return fail(ALE_B200_E_ARG, "ale: domain too large for 32-bit offsets");
     if (a->method == 4 || a->method == 5)
         return fail(ALE_B200_E_UNSUPPORTED, "ale: REMAP_PPM_H4 and REMAP_PQM are not implemented");
     if (!a->h_layer || !a->mass_budget || !a->bt_eta || !a->bt_H_ref || !a->dsig || !a->h_old || !a->target_h)
