@@ -766,14 +766,15 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
 // possible for sweep-produced coefficients) is counted in the device error
 // word and skipped.
 // ---------------------------------------------------------------------------
-template <int NT, int CH, class P, class LD>
+// U sublayers are fetched per batch; the best depth depends on the kernel's
+// register budget (the standalone gather uses 3, the persistent kernel 4).
+template <int NT, int CH, class P, class LD, int U = 4>
 __device__ __forceinline__ void gather_run(const typename P::Flux* const (&F)[NT],
                                            const typename P::Ko* __restrict__ KoS, size_t stride, bool left, int ns,
                                            int& ptr, int k0, int k1, double (&dTr)[NT][CH], int& bad) {
     // Sublayers are fetched U at a time (independent loads in flight), then
     // consumed in order until the first one beyond the chunk. The per-layer
     // sums stay in registers (see below).
-    constexpr int U = 4;
     int s = ptr;
     while (s < ns - 1) {
         int kk[U];
@@ -820,7 +821,7 @@ __device__ __forceinline__ void gather_run(const typename P::Flux* const (&F)[NT
     ptr = s;
 }
 
-template <int NT, int CH, class P, class LD>
+template <int NT, int CH, class P, class LD, int U = 4>
 // Tracers tr0 .. tr0+NT-1 of the state; their fluxes sit at slots
 // fslot .. fslot+NT-1 of the flux buffer.
 __device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, int j, int tr0, int fslot) {
@@ -860,7 +861,8 @@ __device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, 
             for (int n = 0; n < NT; ++n)
                 F[n] = (u ? a.Fu : a.Fv) + (size_t)(fslot + (n < nt ? n : 0)) * (size_t)(ns - 1) * stride + fo[f];
             const FaceInT<P>& c = u ? a.u : a.v;
-            gather_run<NT, CH, P, LD>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1, dTr, bad);
+            gather_run<NT, CH, P, LD, U>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1, dTr,
+                                         bad);
         }
         // Layers k0..k1-1 are complete: hTr(knat) += dTr(knat) * (1/areaT), knat = nz + 1 - k.
 #pragma unroll
