@@ -277,7 +277,7 @@ Profiler g_prof;
 namespace redi {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-static CellTuning g_cell_tuning{32, 4, 8, 8};
+static CellTuning g_cell_tuning{64, 2, 4, 8};  // the autotuner's usual choice at config 1
 CellTuning cell_tuning() { return g_cell_tuning; }
 void set_cell_tuning(const CellTuning& t) { g_cell_tuning = t; }
 

@@ -767,7 +767,8 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
 // word and skipped.
 // ---------------------------------------------------------------------------
 // U sublayers are fetched per batch; the best depth depends on the kernel's
-// register budget (the standalone gather uses 3, the persistent kernel 4).
+// register budget (the standalone gather uses 3 with 4-layer chunks and 4 with
+// deeper ones, the persistent kernel 4).
 template <int NT, int CH, class P, class LD, int U = 4>
 __device__ __forceinline__ void gather_run(const typename P::Flux* const (&F)[NT],
                                            const typename P::Ko* __restrict__ KoS, size_t stride, bool left, int ns,

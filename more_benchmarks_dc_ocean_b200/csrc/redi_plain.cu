@@ -76,7 +76,8 @@ __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0, 
 template <int NT, int CH, class P>
 __global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgsT<P> a, int tr0, int fslot, int j0, int j1) {
     const int j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
-    if (j < j1) gather_item<NT, CH, P, LdNC, 3>(a, blockIdx.x * blockDim.x + threadIdx.x, j, tr0, fslot);
+    // sublayers fetched per round trip: 3 with 4-layer chunks, 4 with deeper chunks (measured)
+    if (j < j1) gather_item<NT, CH, P, LdNC, (CH <= 4 ? 3 : 4)>(a, blockIdx.x * blockDim.x + threadIdx.x, j, tr0, fslot);
 }
 
 // The point EOS at n independent points, as the column state evaluates it at
