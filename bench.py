@@ -4,7 +4,7 @@
                     [--config config1|config3|config0|config4] [--precision fp64|mixed]
 
 One step = redi_calc_coeffs + redi_apply_flux over every tracer of the domain.
-Metric: tracer-cell updates/s = N_tracers * nx_phys * ny_phys * nz
+Metric (the reference's headline): tracer-cell updates/s = N_tracers * nx_phys * ny_phys * nz
 / t_step, land cells included; `value` sums all ranks.
 
 * value: inputs resident in HBM, K steps timed with CUDA events on the

@@ -94,7 +94,7 @@ def reference_ic(nxp: int = 473, nyp: int = 297, nz: int = 30, nghost: int = 3) 
     a["rho_layer"][:] = (1025.0 + 5.0 * (nz - k) / nz)[:, None, None]
     i = np.arange(1, nx + 1)
     j = np.arange(1, ny + 1)
-    # C integer division of the point counts, as the driver writes them
+    # C integer division of the point counts, as the reference's meke/drivers/cpp_main.cu writes them
     ga = (i - nx // 2).astype(np.float64) / max(nx // 6, 1)
     gb = (j - ny // 2).astype(np.float64) / max(ny // 6, 1)
     a["gm_src"][:] = 1.0e-2 * np.exp(-(ga[None, :] ** 2 + gb[:, None] ** 2))
