@@ -12,10 +12,15 @@
 // multiplication; a Fortran compiler that folds x**n with a single rounding
 // can differ from these in the last bit of a few coefficients, so bit parity
 // with the Fortran itself is unpinned (no Fortran compiler in this image).
-// The restatement is pinned instead by (a) finite-difference consistency of
-// dSV/dT and dSV/dS with SV (the check the reference's comments name,
-// ocean_eos.F90:300-306), (b) plausible seawater densities, and (c) bit
-// equality with the independently written device code.
+// wright_dsv is pinned bit for bit against the reference's own CUDA
+// transcriptions of eos_specvol_derivs (epbl/epbl_kernel.cu:112-137,
+// kappa_shear/ks_kernel.cu:108-134; golden vectors
+// tests/golden/eos_specvol_ref.npz, 2318 points, 0 ulp). wright_rho and the
+// Roquet branch have no compiled counterpart in the reference and are pinned
+// by (a) finite-difference consistency of dSV/dT and dSV/dS with SV (the check
+// the reference's comments name, ocean_eos.F90:300-306), (b) plausible
+// seawater densities, and (c) bit equality with the independently written
+// device code.
 #pragma once
 
 #include <cmath>

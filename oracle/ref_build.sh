@@ -64,3 +64,24 @@ fi
 if [[ -f "$REF/ale_remap/ale_kernel.cu" ]]; then
   build_pair ale "$REF/ale_remap" -DMODEL_NZ_STACK_MAX=128 -- ale_kernel.cu opt_kernel.cu
 fi
+
+# The reference's CUDA transcriptions of eos_specvol_derivs (WRIGHT_97 and
+# LINEAR), one per model that carries one, run through oracle/ref_eos_harness.cu
+# (built with each model's own size definitions, FMA contraction off).
+build_eos() {
+  local name="$1" dir="$2" macro="$3" src="$4"; shift 4
+  local lib="$OUT/libeos_${name}_refcuda.so"
+  if [[ -f "$lib" && "$lib" -nt "$dir/$src" && "$lib" -nt "$HERE/ref_eos_harness.cu" && "$lib" -nt "$0" ]]; then
+    return 0
+  fi
+  "$NVCC" -O3 "${ARCH[@]}" -fmad=false -I"$REF/common" -I"$dir" --compiler-options -fPIC "$@" -D"$macro" \
+    -shared "$HERE/ref_eos_harness.cu" -o "$lib"
+  echo "built $lib"
+}
+if [[ -f "$REF/epbl/epbl_kernel.cu" ]]; then
+  build_eos epbl "$REF/epbl" REF_EOS_EPBL epbl_kernel.cu \
+    -DMODEL_NZ_STACK_MAX=128 -DEPBL_LB_THREADS=128 -DEPBL_LB_BLOCKS_PER_SM=4
+fi
+if [[ -f "$REF/kappa_shear/ks_kernel.cu" ]]; then
+  build_eos ks "$REF/kappa_shear" REF_EOS_KS ks_kernel.cu -DMODEL_NZ_STACK_MAX=128 -DKS_FULL_COPY
+fi

@@ -9,6 +9,8 @@ through whole steps (coefficients and tracers), alone and inside the
 multi-domain batch.
 """
 
+import os
+
 import numpy as np
 import pytest
 
@@ -46,6 +48,24 @@ def test_eos_points_match_oracle(redi_lib, oracle_lib, variant):
     ref = np.array([O.eos_point(oe, a, b, c) for a, b, c in zip(T, S, p)])
     for name, got, want in (("rho", rho, ref[:, 0]), ("dsv_dt", dT, ref[:, 1]), ("dsv_ds", dS, ref[:, 2])):
         assert np.array_equal(got, want), f"variant {variant} {name}: {np.count_nonzero(got != want)} differ"
+
+
+@pytest.mark.parametrize("variant,name", [(1, "linear"), (2, "wright")])
+def test_eos_points_match_reference_cuda(redi_lib, variant, name):
+    """dSV/dT and dSV/dS against the reference's own CUDA eos_specvol_derivs
+    (epbl/epbl_kernel.cu:112-137 and kappa_shear/ks_kernel.cu:108-134, fixture
+    tests/golden/eos_specvol_ref.npz), 0 ulp."""
+    R = redi_lib
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "eos_specvol_ref.npz"))
+    e = R.OceanEos(variant=variant, rho0=float(z["cfg_rho0"]), alpha_T=float(z["cfg_alpha_T"]),
+                   beta_S=float(z["cfg_beta_S"]))
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    _, dT, dS = R.eos_points(e, d(z["T"]), d(z["S"]), d(z["p"]))
+    torch.cuda.synchronize()
+    for dname, got in (("dsv_dt", dT.cpu().numpy()), ("dsv_ds", dS.cpu().numpy())):
+        for copy in ("epbl", "ks"):
+            want = z[f"{copy}_{name}_{dname}"]
+            assert np.array_equal(got, want), f"{copy} {dname}: {np.count_nonzero(got != want)} differ"
 
 
 def _problem(variant, seed=31):

@@ -1,13 +1,20 @@
 """The oracle's point equation of state: the non-linear branches of redi/ocean_eos.F90.
 
-The reference's WRIGHT_97 and ROQUET_SPV branches live only in its Fortran, which
-cannot be compiled here, and its CUDA implements the linear branch only, so no
-reference output pins them. They are pinned by what the reference itself uses
-to check them (ocean_eos.F90:300-306, 516-525): the specific-volume derivatives
-must equal finite differences of the specific volume, densities must be those
-of seawater, and the two independent fits (Wright 1997, Roquet 2015) must agree
-over the oceanic range.
+The reference's Redi CUDA implements the linear branch only, and its Fortran
+cannot be compiled here. The WRIGHT_97 specific-volume derivatives are pinned
+bit for bit against the reference's own CUDA transcriptions of
+eos_specvol_derivs in two other models (epbl/epbl_kernel.cu:112-137,
+kappa_shear/ks_kernel.cu:108-134), run on a B200 by
+tests/golden/make_eos_golden.py (fixture eos_specvol_ref.npz). The WRIGHT_97
+density and the ROQUET_SPV branch exist in no compiled form of the reference;
+they are pinned by what the reference itself uses to check them
+(ocean_eos.F90:300-306, 516-525): the specific-volume derivatives must equal
+finite differences of the specific volume, densities must be those of seawater,
+and the two independent fits (Wright 1997, Roquet 2015) must agree over the
+oceanic range.
 """
+
+import os
 
 import numpy as np
 import pytest
@@ -16,6 +23,7 @@ from more_benchmarks_dc_ocean_b200.inputs import Eos
 from oracle import oracle as O
 
 WRIGHT, ROQUET = 2, 4
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "eos_specvol_ref.npz")
 POINTS = [(T, S, p) for T in (-1.5, 2.0, 10.0, 18.0, 29.0) for S in (30.0, 34.7, 35.0, 37.5)
           for p in (0.0, 1.0e7, 4.0e7)]
 
@@ -67,3 +75,16 @@ def test_linear_variant_codes(oracle_lib):
         a, b = O.eos_point(e1, T, S, p), O.eos_point(e0, T, S, p)
         assert a == b
         assert a[0] == 1035.0 + 7.6e-4 * (S - 35.0) - 2e-4 * (T - 10.0)
+
+
+@pytest.mark.parametrize("copy", ["epbl", "ks"])
+@pytest.mark.parametrize("variant,name", [(1, "linear"), (WRIGHT, "wright")])
+def test_specvol_derivs_match_reference_cuda(oracle_lib, copy, variant, name):
+    """dSV/dT and dSV/dS at 2318 points, 0 ulp against each reference CUDA copy."""
+    z = np.load(GOLDEN)
+    e = Eos(variant=variant, rho0=float(z["cfg_rho0"]), alpha_T=float(z["cfg_alpha_T"]),
+            beta_S=float(z["cfg_beta_S"]))
+    got = np.array([O.eos_point(e, a, b, c)[1:] for a, b, c in zip(z["T"], z["S"], z["p"])])
+    for i, d in enumerate(("dsv_dt", "dsv_ds")):
+        want = z[f"{copy}_{name}_{d}"]
+        assert np.array_equal(got[:, i], want), f"{d}: {np.count_nonzero(got[:, i] != want)} of {want.size} differ"

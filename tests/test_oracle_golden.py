@@ -1,7 +1,8 @@
 """The CPU oracle against golden vectors produced by the reference's own CUDA.
 
 Each Redi fixture in tests/golden/*.npz (the meke_* and ale_* fixtures belong to
-the MEKE and ALE remap steps, test_meke_cpu.py and test_ale_cpu.py) holds seeded
+the MEKE and ALE remap steps, test_meke_cpu.py and test_ale_cpu.py, and the eos_*
+fixture to the point EOS, test_oracle_eos.py) holds seeded
 inputs and the outputs of the
 reference launcher `redi_opt_launch` (redi/opt_kernel.cu, built from the
 reference sources with FMA contraction off; see tests/golden/make_golden.py):
@@ -18,7 +19,7 @@ import pytest
 from more_benchmarks_dc_ocean_b200.inputs import Eos, RediProblem
 
 GOLDEN = sorted(g for g in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(g).startswith(("meke_", "ale_")))
+                if not os.path.basename(g).startswith(("meke_", "ale_", "eos_")))
 
 
 def _problem(z) -> RediProblem:
