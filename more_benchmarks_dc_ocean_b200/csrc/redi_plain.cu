@@ -56,8 +56,8 @@ __global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a, int c0,
 
 template <class P>
 __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgsT<P> a, FaceRange r) {
-    const int d = blockIdx.y;
-    const int t = r.lo[d] + blockIdx.x * blockDim.x + threadIdx.x;
+    const int d = blockIdx.x & 1;  // blocks alternate between u and v faces, as in k_face_flux
+    const int t = r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
     if (t < r.hi[d]) sweep_item<P, LdNC, true>(a, d, t);
 }
 
@@ -67,10 +67,13 @@ __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgsT<P> a, int c0, i
 }
 
 // Every thread of the block reaches flux_item (its warp-wide votes need all lanes).
+// Blocks alternate between the directions (even: u faces, odd: v faces), so the
+// u and v faces of the same rows are in flight together and the second reads of
+// a column's reconstruction are served from L2 instead of HBM.
 template <int NT, class P>
 __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0, FaceRange r) {
-    const int d = blockIdx.y;
-    flux_item<NT, P, LdNC>(a, d, r.lo[d] + blockIdx.x * blockDim.x + threadIdx.x, tr0, r.hi[d]);
+    const int d = blockIdx.x & 1;
+    flux_item<NT, P, LdNC>(a, d, r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x, tr0, r.hi[d]);
 }
 
 template <int NT, int CH, class P>
@@ -160,7 +163,7 @@ cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st, Band band) {
     if (nb > 0) {
         const int kid = P::kMixed ? K_MIXED_SWEEP : K_NEUTRAL_SWEEP;
         launch_begin(kid, st);
-        plain::k_neutral_sweep<P><<<dim3(nb, 2), 128, 0, st>>>(sw, r.f);
+        plain::k_neutral_sweep<P><<<2 * nb, 128, 0, st>>>(sw, r.f);
         launch_end(kid, st);
     }
     return cudaGetLastError();
@@ -175,7 +178,7 @@ static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT
     if (nb > 0) {
         const int kid = P::kMixed ? K_MIXED_FLUX : K_FACE_FLUX;
         launch_begin(kid, st);
-        plain::k_face_flux<NT, P><<<dim3(nb, 2), 128, 0, st>>>(ff, tr0, r.f);
+        plain::k_face_flux<NT, P><<<2 * nb, 128, 0, st>>>(ff, tr0, r.f);
         launch_end(kid, st);
     }
     if (cgrid.y == 0) return;
