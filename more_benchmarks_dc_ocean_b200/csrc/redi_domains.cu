@@ -282,6 +282,19 @@ DomainKernel<P> kernel_for(int chunk, int occ) {
     }
 }
 
+// Queue position p of a face stage's ntiles tiles -> tile index (tiles < nu are
+// u faces): u and v tiles alternate while both remain, so the two directions of
+// the same rows are in flight together and a column's data is read from HBM once.
+inline int face_tile_at(int p, int nu, int ntiles) {
+    const int nv = ntiles - nu, m = nu < nv ? nu : nv;
+    if (p < 2 * m) return (p & 1) ? nu + (p >> 1) : (p >> 1);
+    return nu > nv ? p - m : nu + (p - m);
+}
+
+inline bool face_stage(int st) {
+    return st == redi::domains::S_SWEEP || (st >= redi::domains::S_PAIR0 && ((st - redi::domains::S_PAIR0) & 1) == 0);
+}
+
 // Gather tiling, work queue and persistent grid for the current launch shape.
 template <class P>
 int layout(redi_b200_batch* b) {
@@ -301,7 +314,9 @@ int layout(redi_b200_batch* b) {
     for (int st = 0; st < kMaxStages; ++st)
         for (int k : order)
             if (st < hd[k].nstages)
-                for (int t = 0; t < hd[k].ntiles[st]; ++t) q.push_back(Item{(int16_t)k, (int16_t)st, t});
+                for (int t = 0; t < hd[k].ntiles[st]; ++t)
+                    q.push_back(Item{(int16_t)k, (int16_t)st,
+                                     face_stage(st) ? face_tile_at(t, hd[k].nu_tiles, hd[k].ntiles[st]) : t});
     drop_graph(b);
     if (b->d_queue) cudaFree(b->d_queue);
     b->d_queue = nullptr;
