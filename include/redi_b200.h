@@ -153,7 +153,10 @@ REDI_B200_API int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b2
  * nbands bands of rows (1..64): rows are copied up on one stream, each band
  * is stepped as soon as its rows and the next row are on the device, and
  * finished rows are copied back on a third stream, so host<->device traffic
- * overlaps the kernels and itself. Results equal the two device entry points
+ * overlaps the kernels and itself. With nbands >= 3 and at least 4 rows per
+ * band the last two bands are a half and a quarter of the others (the last
+ * band's kernels and download start only when every row is up, so a short
+ * last band shortens the step). Results equal the two device entry points
  * bit for bit. Stream-ordered on `stream`: the host arrays are in use until
  * the stream reaches this call's end; page-locked host memory is needed for
  * the copies to overlap. Each phase keeps its own gates; SKIPPED when both

@@ -647,6 +647,20 @@ int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* me
 
 }  // extern "C"
 
+// First row of band b of nbands over ny rows (b == nbands gives ny). With
+// nbands >= 3 and ny >= 4 nbands the bands weigh 1, ..., 1, 1/2, 1/4 (in
+// quarters: 4, ..., 4, 2, 1; total 4 nbands - 5 <= ny, so every band has a
+// row): the last band's kernels and download wait for the last upload, and a
+// short last band shortens that tail. Otherwise the bands are equal.
+static int band_edge(int b, int nbands, int ny) {
+    if (nbands >= 3 && ny >= 4 * nbands) {
+        const long long total = 4LL * nbands - 5;
+        const long long acc = b <= nbands - 2 ? 4LL * b : (b == nbands - 1 ? total - 1 : total);
+        return (int)(acc * ny / total);
+    }
+    return (int)((long long)b * ny / nbands);
+}
+
 // redi_calc_coeffs followed by redi_apply_flux on a model state that lives in
 // host memory, pipelined over bands of rows: rows stream in on one stream,
 // each band is stepped on a second as soon as its rows (and the row after
@@ -695,7 +709,7 @@ int step_host_impl(const redi_b200_grid* grid, const redi_b200_metrics* metrics,
     const double* sh = hp.tin[ms->idx_salinity > 0 ? ms->idx_salinity - 1 : 0];
     int copied = 0;  // rows already on the device
     for (int b = 0; b < nbands; ++b) {
-        const int j0 = (int)((long long)b * ny / nbands), j1 = (int)((long long)(b + 1) * ny / nbands);
+        const int j0 = band_edge(b, nbands, ny), j1 = band_edge(b + 1, nbands, ny);
         const int need = j1 + 1 < ny ? j1 + 1 : ny;  // the band's cells read one row beyond it
         cudaEvent_t up_b = hp.ev[2 + 2 * b], comp_b = hp.ev[3 + 2 * b];
         if (need > copied) {
