@@ -16,6 +16,8 @@ Metric (the reference's headline): tracer-cell updates/s = N_tracers * nx_phys *
   device, runs the step and copies every tracer back. On one GPU this is
   redi_b200_step_host, which pipelines the copies and the kernels over row
   bands; with halo exchange (N > 1) the copies wrap the device entry points.
+  On one GPU the line also carries copy_floor_ms, the same copies alone (up
+  and down concurrently, no kernels), and e2e's fraction of it.
 * roofline: the dominant kernel (most device time in the timed region, from
   CUDA event pairs the library records around each launch on its stream);
   achieved = algorithmic bytes per launch / mean launch time.
@@ -716,6 +718,38 @@ def _max_over_ranks(x, dist, dev):
     return float(t.item())
 
 
+def _copy_floor_ms(host_h, host_tr, dp, st) -> float:
+    """The e2e step's copies alone, with no kernels: h and every tracer up on one
+    stream while every tracer comes down on another (separate buffers), best of
+    3 after one warm-up. The bound the host-state step's pipeline can approach."""
+    import torch
+
+    up_dst = [torch.empty_like(dp.ms.h_layer)] + [torch.empty_like(d) for d in dp.ms.tracers]
+    up_src = [host_h] + list(host_tr)
+    down_dst = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in host_tr]
+    s_up, s_dn = torch.cuda.Stream(), torch.cuda.Stream()
+    ts = []
+    for _ in range(4):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s_up.wait_event(a)
+        s_dn.wait_event(a)
+        with torch.cuda.stream(s_up):
+            for d, h in zip(up_dst, up_src):
+                d.copy_(h, non_blocking=True)
+        with torch.cuda.stream(s_dn):
+            for d, h in zip(dp.ms.tracers, down_dst):
+                h.copy_(d, non_blocking=True)
+        st.wait_stream(s_up)
+        st.wait_stream(s_dn)
+        b.record(st)
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    del up_dst, down_dst
+    return min(ts[1:])
+
+
 def _e2e(args, p, dp, redi, ex, st, dist, dev, world):
     import torch
 
@@ -771,9 +805,14 @@ def _e2e(args, p, dp, redi, ex, st, dist, dev, world):
     torch.cuda.synchronize()
     ms = _max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, dev)
     nt = p.nx * p.ny * p.nz
-    return {"value": p.ntr * p.nx_phys * p.ny_phys * p.nz * world / (ms * 1e-3), "unit": UNIT,
-            "h2d_bytes_per_step": 8 * nt * (1 + p.ntr), "d2h_bytes_per_step": 8 * nt * p.ntr, "ms_per_step": ms,
-            "host_memory": "pinned", "path": path, "band_candidates_ms": band_ms}
+    out = {"value": p.ntr * p.nx_phys * p.ny_phys * p.nz * world / (ms * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": 8 * nt * (1 + p.ntr), "d2h_bytes_per_step": 8 * nt * p.ntr, "ms_per_step": ms,
+           "host_memory": "pinned", "path": path, "band_candidates_ms": band_ms}
+    if ex is None:
+        floor = _copy_floor_ms(host_h, host_tr, dp, st)
+        out["copy_floor_ms"] = floor
+        out["frac_of_copy_floor"] = floor / ms
+    return out
 
 
 # ---------------------------------------------------------------------------
