@@ -18,9 +18,12 @@
 # contraction is off (-fmad=false) so the result is the IEEE sequence of the
 # source, comparable bit for bit. The *_native.so twins keep the reference's
 # own flags (FMA contraction on) and are used only for timing.
+#
+# The reference checkout is $REDI_REFERENCE_DIR, or else a directory named
+# `reference` beside this repository's root.
 set -euo pipefail
-REF="${REDI_REFERENCE_DIR:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${REDI_REFERENCE_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 if [[ ! -f "$REF/redi/redi_kernel.cu" ]]; then
   echo "ref_build.sh: reference sources not found under $REF; skipping" >&2

@@ -8,8 +8,7 @@ compressed .npz fixtures beside this script. tests/test_oracle_golden.py checks
 the CPU oracle against them on any machine.
 
 It also compares the oracle with the reference launchers at the full config-0
-size (10 steps) and prints the agreement; that log is summarised in
-tests/golden/README.md.
+size (10 steps) and prints the agreement.
 
 Usage (on a machine with a CUDA GPU, after oracle/ref_build.sh):
     python tests/golden/make_golden.py [--out DIR] [--config0]
