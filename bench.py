@@ -55,7 +55,8 @@ METRIC = "Redi tracer-cell updates/s, HBM GB/s; mixed+batched vs FP64 plain, 1 B
 UNIT = "tracer-cell updates/s"
 KERNEL_NAMES = ["k_column_state", "k_neutral_sweep", "k_tracer_recon", "k_cell_gather", "k_face_flux",
                 "k_mixed_recon", "k_mixed_flux", "k_mixed_sweep", "k_domain_persistent", "aux",
-                "k_meke_column", "k_meke_del2", "k_meke_lateral", "k_ale_columns", "k_ale_faces"]
+                "k_meke_column", "k_meke_del2", "k_meke_lateral", "k_ale_columns", "k_ale_faces",
+                "k_flux_fold", "k_mixed_fold"]
 NKERN = len(KERNEL_NAMES)
 FALLBACK_HBM_GBS = 6650.0
 
@@ -116,6 +117,8 @@ def kernel_bytes(p, kid: int, precision: str = "fp64") -> float:
         return float(bcoef + face2d)
     if kid == 3:       # cell gather, one launch per tracer pair: read + write its tracers
         return float(16 * s["Nt"] * min(2, s["ntr"]) + 8 * s["ncol"])
+    if kid in (15, 16):  # fused face flux + fold: the coefficients once, every tracer read + written
+        return float(bcoef + face2d + 16 * s["Nt"] * s["ntr"])
     return 0.0
 
 
@@ -422,8 +425,16 @@ def run_b200(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        upd, info = cpu_sample(p, args.cpu_seconds)
-        cpu = {"value": upd, "unit": UNIT, "cores": info["cores"], "kind": "port", "sample": info["sample"]}
+        upd, info = cpu_sample(p, args.cpu_seconds / 3, nsteps=3)
+        cpu = {"value": upd, "unit": UNIT, "cores": info["cores"], "kind": "port",
+               "cores_note": "the threads of this process's CPU affinity set (the lease's cores), one per thread",
+               "sample": info["sample"]}
+
+    # ---- the second half of the metric: mixed precision (config 2) and 34-tracer batching (config 3) ----
+    sub = None
+    if world == 1 and not args.no_sub and args.config == "config1" and args.precision == "fp64" and not args.grid:
+        redi.destroy()
+        sub = _mixed_batched(args, p, dp, st, value)
 
     if rank == 0:
         line = {
@@ -446,6 +457,8 @@ def run_b200(args, rank, world, local_rank):
                        "candidates_ms": tuning["ms"]} if tuning else None,
             "hbm_gbs_per_rank": bstep / (ms_all * 1e-3) / 1e9,
         }
+        if sub is not None:
+            line.update(sub)
         print(json.dumps(line), flush=True)
     redi.destroy()
     if ex is not None:
@@ -454,6 +467,64 @@ def run_b200(args, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _time_steps(dp, redi, st, warmup: int, steps: int) -> float:
+    """ms per Redi step (calc_coeffs + apply_flux of every tracer), CUDA events on the launching stream."""
+    import torch
+
+    from more_benchmarks_dc_ocean_b200 import ocean_redi as R
+
+    for _ in range(warmup):
+        R.step(dp, redi, 1, st)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        R.step(dp, redi, 1, st)
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _mixed_batched(args, p, dp, st, plain_value: float) -> dict:
+    """Sub-records for the mixed+batched half of the metric, measured in this process right after the
+    plain line: config 2 (the same 1440x1080x75 inputs, mixed precision) and config 3 (720x576x50, T, S
+    and 32 passive tracers, mixed precision, every tracer's fluxes in one fused Phase-B launch). Each
+    reports ms per step, tracer-cell updates/s and its ratio to the plain FP64 value of this line."""
+    import torch
+
+    from more_benchmarks_dc_ocean_b200 import inputs
+    from more_benchmarks_dc_ocean_b200 import ocean_redi as R
+
+    out = {}
+    steps, warm = max(3, min(args.steps, 10)), 3
+    redi = R.make_redi(dp, R.MIXED)
+    ms = _time_steps(dp, redi, st, warm, steps)
+    redi.destroy()
+    upd = p.ntr * p.nx_phys * p.ny_phys * p.nz / (ms * 1e-3)
+    out["mixed_c2"] = {"workload": f"config2: mixed-precision Redi step {p.nx_phys}x{p.ny_phys}x{p.nz}, "
+                                   f"{p.ntr} tracers (the inputs of this line)",
+                       "ms_per_step": ms, "value": upd, "unit": UNIT, "steps": steps, "warmup": warm,
+                       "ratio_vs_plain": upd / plain_value}
+    q = inputs.config3()
+    dq = R.to_device(q, torch.device("cuda", torch.cuda.current_device()))
+    redi = R.make_redi(dq, R.MIXED)
+    from more_benchmarks_dc_ocean_b200 import autotune
+
+    group = autotune.tune_tracer_group(dq, redi, stream=st)
+    ms = _time_steps(dq, redi, st, warm, steps)
+    redi.destroy()
+    upd = q.ntr * q.nx_phys * q.ny_phys * q.nz / (ms * 1e-3)
+    out["batched_c3"] = {"workload": f"config3: mixed-precision Redi step {q.nx_phys}x{q.ny_phys}x{q.nz}, "
+                                     f"{q.ntr} tracers; coefficients once per step, every tracer reconstructed in "
+                                     f"one launch, face fluxes in tracer groups of {group['best']} (autotuned)",
+                         "ms_per_step": ms, "value": upd, "unit": UNIT, "steps": steps, "warmup": warm,
+                         "ratio_vs_plain": upd / plain_value, "tracer_group_ms": group["ms"]}
+    autotune.set_tracer_group(8)
+    del dq
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -1293,6 +1364,7 @@ def main():
     ap.add_argument("--grid", default=None, help="NXxNYxNZ: a generated domain of that size instead of --config")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-sub", action="store_true", help="skip the mixed (config 2) and batched (config 3) sub-records")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--domains", type=int, default=64, help="config4: number of regional domains")

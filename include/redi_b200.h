@@ -190,7 +190,8 @@ REDI_B200_API int redi_b200_version(void);
  * update), 4 face_flux, 5 mixed_recon, 6 mixed_flux, 7 mixed_sweep,
  * 8 domain_persistent, 9 auxiliary, and the MEKE step's (meke_b200.h) 10 pass A,
  * 11 biharmonic Laplacian, 12 pass B, and the ALE remap step's (ale_b200.h) 13 column
- * tiles, 14 face tiles; redi_b200_kernel_count() is their number.
+ * tiles, 14 face tiles, then 15 flux_fold and 16 mixed_fold (the fused Phase-B
+ * pass); redi_b200_kernel_count() is their number.
  * redi_b200_launch_count(k) counts launches of kernel k since load (k < 0:
  * all). Between profile_begin and profile_end every launch is bracketed by a
  * CUDA event pair on its own stream; profile_end waits for them and returns,
@@ -217,6 +218,25 @@ REDI_B200_API int redi_b200_eos_points(const redi_b200_eos* eos, int n, const do
  * at higher occupancy; results do not depend on it. */
 REDI_B200_API int redi_b200_set_tracer_group(int max_group);
 REDI_B200_API int redi_b200_get_tracer_group(void);
+/* Phase B as one fused pass per tile of cells (no counterpart in the
+ * reference), process-wide: every face's sublayer fluxes are computed once per
+ * tile and added to the cells' tendencies in shared memory, so no flux buffer
+ * crosses HBM and all tracers go through one launch. enable is a mask: bit 0
+ * runs the FP64 form this way, bit 1 the mixed form, bit 2 makes the mixed form
+ * add in the reference's order too. The FP64 form always adds in the
+ * reference's order (results bit-identical to the face-flux + cell-gather pair
+ * it replaces); the mixed form otherwise adds each term as soon as it is
+ * computed (shared-memory atomics: the same terms, FP64 accumulation, in an
+ * order that can differ from run to run by the last bits). rows: cell rows per
+ * tile (1 or 2); tracers: tracers per pass (1, 2, 4, or 0 for the most that
+ * keep two tiles per SM). Off by default (the pair runs; rows = 2).
+ * redi_b200_fold_shape reports the (rows, tracers) a step of the given
+ * precision, nz and tracer count runs with; tracers = 0 means the pair runs
+ * (the fused pass is off for that form, or its shared memory would not fit:
+ * very deep columns). Kernel ids 15 (FP64) and 16 (mixed) time it. */
+REDI_B200_API int redi_b200_set_fold(int enable, int rows, int tracers);
+REDI_B200_API int redi_b200_get_fold(int* enable, int* rows, int* tracers);
+REDI_B200_API int redi_b200_fold_shape(int precision, int nz, int ntracers, int* rows, int* tracers);
 REDI_B200_API unsigned long long redi_b200_launch_count(int kernel);
 REDI_B200_API int redi_b200_profile_begin(void);
 REDI_B200_API int redi_b200_profile_end(double* total_ms, unsigned long long* counts, int n);
@@ -266,7 +286,13 @@ REDI_B200_API void redi_cuda_launch_(const int* nx, const int* ny, const int* nz
  * any stream capture. A domain whose scratch exceeds 64 MiB (about 18 000
  * columns at nz = 25, 6 000 at nz = 75) is refused with
  * REDI_B200_E_UNSUPPORTED; the message (redi_b200_last_error) gives the
- * limit. Returns REDI_B200_OK or a negative status. */
+ * limit. The array pointers are checked as redi_opt_launch checks them
+ * (doubles 8-byte, the int Ko slots 4-byte aligned). Its Phase B uses the
+ * coefficients its own Phase A just made, which are never out of order, so no
+ * out-of-order count is kept for it (redi_b200_error_count is per handle).
+ * The device address of the array is cached per device index for the life of
+ * the process: do not call it again on a device after cudaDeviceReset.
+ * Returns REDI_B200_OK or a negative status. */
 REDI_B200_API int redi_b200_opt_launch_noalloc(
     const int* nx, const int* ny, const int* nz, const int* ns, const double* dt, const int* nghost, const int* nxp,
     const int* nyp, const int* ww, const int* we, const int* wsz, const int* wn, const double* rho0,

@@ -59,6 +59,43 @@ def set_tracer_group(max_group: int) -> None:
     R._check(L.redi_b200_set_tracer_group(int(max_group)))
 
 
+FOLD_FP64, FOLD_MIXED, FOLD_MIXED_ORDERED = 1, 2, 4
+
+
+def set_fold(enable: int = FOLD_FP64, rows: int = 2, tracers: int = 0) -> None:
+    """Phase B as the fused face-flux + fold pass or the face-flux / cell-gather pair. enable is a
+    mask: FOLD_FP64 (the FP64 form), FOLD_MIXED (the mixed form, in any order), FOLD_MIXED_ORDERED
+    (the mixed form in the reference's order); True means FOLD_FP64. rows: cell rows per tile
+    (1, 2); tracers per pass (1, 2, 4, 0 = automatic)."""
+    from . import ocean_redi as R
+
+    L = R.lib()
+    L.redi_b200_set_fold.argtypes = [C.c_int, C.c_int, C.c_int]
+    R._check(L.redi_b200_set_fold(int(enable), int(rows), int(tracers)))
+
+
+def get_fold() -> Tuple[int, int, int]:
+    """(enable mask, rows, tracers)."""
+    from . import ocean_redi as R
+
+    L = R.lib()
+    L.redi_b200_get_fold.argtypes = [C.POINTER(C.c_int)] * 3
+    e, r, t = C.c_int(), C.c_int(), C.c_int()
+    R._check(L.redi_b200_get_fold(C.byref(e), C.byref(r), C.byref(t)))
+    return e.value, r.value, t.value
+
+
+def fold_shape(precision: int, nz: int, ntracers: int) -> Tuple[int, int]:
+    """(rows, tracers per pass) the fused pass runs with; tracers == 0: the pair runs."""
+    from . import ocean_redi as R
+
+    L = R.lib()
+    L.redi_b200_fold_shape.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    r, t = C.c_int(), C.c_int()
+    R._check(L.redi_b200_fold_shape(int(precision), int(nz), int(ntracers), C.byref(r), C.byref(t)))
+    return r.value, t.value
+
+
 def get_tracer_group() -> int:
     from . import ocean_redi as R
 
@@ -157,9 +194,9 @@ def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, int, int]]] = None, 
         L.redi_b200_profile_begin()
         for _ in range(reps):
             R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, stream)
-        kt = (C.c_double * 16)()
-        kc = (C.c_ulonglong * 16)()
-        L.redi_b200_profile_end(kt, kc, 16)
+        kt = (C.c_double * R.lib().redi_b200_kernel_count())()
+        kc = (C.c_ulonglong * R.lib().redi_b200_kernel_count())()
+        R._check(L.redi_b200_profile_end(kt, kc, len(kt)))
         kid = K_CELL_UPDATE
         times[cand] = kt[kid] / max(1, kc[kid])
     best = min(times, key=times.get)
@@ -196,9 +233,9 @@ def tune_batch(batch, candidates: Optional[Iterable[Tuple[int, int, int]]] = Non
         torch.cuda.synchronize()
         L.redi_b200_profile_begin()
         batch.step(reps, stream)
-        kt = (C.c_double * 16)()
-        kc = (C.c_ulonglong * 16)()
-        L.redi_b200_profile_end(kt, kc, 16)
+        kt = (C.c_double * R.lib().redi_b200_kernel_count())()
+        kc = (C.c_ulonglong * R.lib().redi_b200_kernel_count())()
+        R._check(L.redi_b200_profile_end(kt, kc, len(kt)))
         times[cand] = kt[K_DOMAIN_PERSISTENT] / max(1, kc[K_DOMAIN_PERSISTENT])
     best = min(times, key=times.get)
     batch.set_tuning(best[:2], best[2], best[3] if len(best) > 3 else 0)

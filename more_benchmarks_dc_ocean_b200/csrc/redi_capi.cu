@@ -280,6 +280,9 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 static CellTuning g_cell_tuning{64, 2, 4, 8};  // the autotuner's usual choice at config 1
 CellTuning cell_tuning() { return g_cell_tuning; }
 void set_cell_tuning(const CellTuning& t) { g_cell_tuning = t; }
+static FoldTuning g_fold_tuning{0, 2, 0, 0, 0};  // the pair stays the default until the fused pass is faster
+FoldTuning fold_tuning() { return g_fold_tuning; }
+void set_fold_tuning(const FoldTuning& t) { g_fold_tuning = t; }
 
 void launch_begin(int kid, cudaStream_t st) {
     std::lock_guard<std::mutex> lock(g_prof.mu);
@@ -385,6 +388,33 @@ int redi_b200_set_tracer_group(int max_group) {
 }
 
 int redi_b200_get_tracer_group(void) { return redi::cell_tuning().group; }
+
+int redi_b200_set_fold(int enable, int rows, int tracers) {
+    if (rows != 1 && rows != 2) return fail(REDI_B200_E_ARG, "redi_b200_set_fold: rows must be 1 or 2");
+    if (tracers != 0 && tracers != 1 && tracers != 2 && tracers != 4)
+        return fail(REDI_B200_E_ARG, "redi_b200_set_fold: tracers must be 0 (automatic), 1, 2 or 4");
+    if (enable < 0 || enable > 7) return fail(REDI_B200_E_ARG, "redi_b200_set_fold: enable is a mask of bits 0..2");
+    redi::set_fold_tuning(redi::FoldTuning{enable & 1, rows, tracers, (enable >> 1) & 1, (enable >> 2) & 1});
+    return REDI_B200_OK;
+}
+
+int redi_b200_get_fold(int* enable, int* rows, int* tracers) {
+    if (!enable || !rows || !tracers) return fail(REDI_B200_E_ARG, "redi_b200_get_fold: NULL argument");
+    const redi::FoldTuning t = redi::fold_tuning();
+    *enable = t.enable | (t.enable_mixed << 1) | (t.ordered_mixed << 2);
+    *rows = t.rows;
+    *tracers = t.tracers;
+    return REDI_B200_OK;
+}
+
+int redi_b200_fold_shape(int precision, int nz, int ntracers, int* rows, int* tracers) {
+    if (!rows || !tracers || nz < 1 || ntracers < 1) return fail(REDI_B200_E_ARG, "redi_b200_fold_shape: bad argument");
+    const redi::FoldShape s = precision == REDI_B200_MIXED ? redi::fold_shape<redi::MixedPrec>(nz, ntracers)
+                                                           : redi::fold_shape<redi::PlainPrec>(nz, ntracers);
+    *rows = s.by;
+    *tracers = s.nt;
+    return REDI_B200_OK;
+}
 
 int redi_b200_eos_points(const redi_b200_eos* eos, int n, const double* T, const double* S, const double* p,
                          double* rho, double* dsv_dt, double* dsv_ds, void* stream) {

@@ -179,7 +179,9 @@ enum KernelId : int {
     K_MEKE_LATERAL = 12,  // MEKE pass B
     K_ALE_COLUMNS = 13,   // ALE remap: targets, snapshot, tracers and the commit
     K_ALE_FACES = 14,     // ALE remap: face velocities
-    K_NUM = 15
+    K_FLUX_FOLD = 15,     // Phase B fused face flux + fold (FP64)
+    K_MIXED_FOLD = 16,    // Phase B fused face flux + fold (mixed)
+    K_NUM = 17
 };
 
 // Sets the message redi_b200_last_error() returns on the calling thread.
@@ -202,6 +204,25 @@ struct CellTuning {
 };
 CellTuning cell_tuning();
 void set_cell_tuning(const CellTuning& t);
+
+// Phase B as one fused face-flux + fold pass (redi_fold.cuh) instead of the
+// face-flux / cell-gather pair: enable, tile rows (1 or 2) and tracers per
+// pass (1, 2, 4; 0 picks the most that keep two blocks per SM), per form
+// (plain FP64, mixed); ordered_mixed: the mixed form folds in the reference's
+// order too (otherwise in any order, through shared-memory atomics).
+struct FoldTuning {
+    int enable, rows, tracers;
+    int enable_mixed, ordered_mixed;
+};
+FoldTuning fold_tuning();
+void set_fold_tuning(const FoldTuning& t);
+// Tile rows and tracers per pass of the fused pass for a problem; nt == 0:
+// it is off or its shared memory does not fit, and the pair runs.
+struct FoldShape {
+    int nt, by;
+};
+template <class P>
+FoldShape fold_shape(int nz, int ntr);
 
 // A band of T-cell rows [row0, row1) of the domain (row1 < 0: to the last
 // row). A step restricted to a band touches the u faces of its rows, the v

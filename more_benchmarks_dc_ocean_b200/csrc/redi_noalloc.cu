@@ -20,7 +20,13 @@
 // different streams or from different host threads without ordering) race on
 // it and corrupt each other's results; issue them in stream order. The array
 // keeps the last call's contents; the only part that must start at zero, the
-// error word, is cleared on the caller's stream by every call.
+// error words, is cleared on the caller's stream by every call. (The words
+// count coefficients found out of order; this entry point makes its own
+// coefficients in Phase A, where that never happens, so it reports none.)
+//
+// The address is cached per device index for the life of the process: after
+// cudaDeviceReset the module is loaded again at a new address, so do not reset
+// a device that this library has stepped on and then call it again.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -91,11 +97,16 @@ int redi_b200_opt_launch_noalloc(const int* nx_, const int* ny_, const int* nz_,
                              rho0_, T_ref_, S_ref_, alpha_T_, beta_S_};
     for (const void* p : scalars)
         if (!p) return set_error(REDI_B200_E_ARG, "NULL scalar argument");
-    const void* arrays[] = {h_layer, t_htr, s_htr, wet_u, wet_v, uPoL, uPoR, uKoL, uKoR, uhEff, vPoL, vPoR,
-                            vKoL, vKoR, vhEff, khtr_u_ext, khtr_v_ext, khtr_u, khtr_v, dy_cu, dx_cv, idxCu,
-                            idyCv, areaT};
-    for (const void* p : arrays)
-        if (!p || (reinterpret_cast<uintptr_t>(p) % 8) != 0) return set_error(REDI_B200_E_ARG, "NULL or misaligned array");
+    // the same checks as redi_opt_launch: doubles 8-byte aligned, the int Ko slots 4-byte aligned
+    const void* reals[] = {h_layer, t_htr, s_htr, wet_u, wet_v, uPoL, uPoR, uhEff, vPoL, vPoR, vhEff,
+                           khtr_u_ext, khtr_v_ext, khtr_u, khtr_v, dy_cu, dx_cv, idxCu, idyCv, areaT};
+    for (const void* p : reals)
+        if (!p || (reinterpret_cast<uintptr_t>(p) % alignof(double)) != 0)
+            return set_error(REDI_B200_E_ARG, "NULL or misaligned array");
+    const void* ints[] = {uKoL, uKoR, vKoL, vKoR};
+    for (const void* p : ints)
+        if (!p || (reinterpret_cast<uintptr_t>(p) % alignof(int)) != 0)
+            return set_error(REDI_B200_E_ARG, "NULL or misaligned array");
     const int nx = *nx_, ny = *ny_, nz = *nz_, ns = *ns_;
     if (nx < 1 || ny < 1 || nz < 1 || nz > redi::kNzMax) return set_error(REDI_B200_E_ARG, "invalid domain extents");
     if (ns != 2 * nz + 2) return set_error(REDI_B200_E_ARG, "ns must equal 2*nz+2");
@@ -121,7 +132,7 @@ int redi_b200_opt_launch_noalloc(const int* nx_, const int* ny_, const int* nz_,
     char* data = static_cast<char*>(base) + kHeader;
     int* err = static_cast<int*>(base);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
+    cudaError_t e = cudaMemsetAsync(err, 0, 2 * sizeof(int), st);
 
     // Phase A (redi_calc_coeffs).
     redi::EosParams eos{1, *rho0_, *T_ref_, *S_ref_, *alpha_T_, *beta_S_};  // the launcher's LINEAR EOS

@@ -35,6 +35,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "redi_fold.cuh"
 #include "redi_items.cuh"
 
 namespace redi {
@@ -202,10 +203,132 @@ static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT
     }
 }
 
+// ---------------------------------------------------------------------------
+// The fused face-flux + fold pass (redi_fold.cuh).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kFoldSmemMax = 232448;      // dynamic shared memory a block may opt into on sm_100a
+constexpr size_t kFoldSmemTwo = 113 * 1024;  // two blocks per SM
+
+template <int NT, class P, int BY, bool ORD>
+cudaError_t launch_fold_o(const fold::FoldArgsT<P>& fa, int jlo, int jhi, cudaStream_t st) {
+    using L = fold::FoldLayout<P, NT, BY, ORD>;
+    const size_t smem = L::bytes(fa.nz);
+    // opt into large dynamic shared memory once per device
+    static int opted[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !opted[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fold::k_flux_fold<NT, P, BY, ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kFoldSmemMax);
+        if (e != cudaSuccess) return e;
+        opted[dev] = 1;
+    }
+    if (fa.abort) {
+        cudaError_t e = cudaMemsetAsync(fa.abort, 0, sizeof(int), st);
+        if (e != cudaSuccess) return e;
+    }
+    const dim3 grid((unsigned)((fa.nx + fold::kTileW - 1) / fold::kTileW), (unsigned)((jhi - jlo + BY - 1) / BY));
+    const int kid = P::kMixed ? K_MIXED_FOLD : K_FLUX_FOLD;
+    launch_begin(kid, st);
+    fold::k_flux_fold<NT, P, BY, ORD><<<grid, 32 * (2 * BY + 1), smem, st>>>(fa, jlo, jhi);
+    launch_end(kid, st);
+    return cudaGetLastError();
+}
+
+// The plain form always folds in the reference's order; the mixed form folds
+// in any order unless the ordered fold is asked for.
+template <int NT, class P, int BY>
+cudaError_t launch_fold_t(const fold::FoldArgsT<P>& fa, int jlo, int jhi, cudaStream_t st) {
+    if (P::kMixed && !fold_tuning().ordered_mixed) return launch_fold_o<NT, P, BY, false>(fa, jlo, jhi, st);
+    return launch_fold_o<NT, P, BY, true>(fa, jlo, jhi, st);
+}
+
+template <class P, bool ORD>
+size_t fold_smem_o(int nt, int by, int nz) {
+    if (by == 1) {
+        return nt == 4 ? fold::FoldLayout<P, 4, 1, ORD>::bytes(nz)
+             : nt == 2 ? fold::FoldLayout<P, 2, 1, ORD>::bytes(nz) : fold::FoldLayout<P, 1, 1, ORD>::bytes(nz);
+    }
+    return nt == 4 ? fold::FoldLayout<P, 4, 2, ORD>::bytes(nz)
+         : nt == 2 ? fold::FoldLayout<P, 2, 2, ORD>::bytes(nz) : fold::FoldLayout<P, 1, 2, ORD>::bytes(nz);
+}
+template <class P>
+size_t fold_smem(int nt, int by, int nz) {
+    return (P::kMixed && !fold_tuning().ordered_mixed) ? fold_smem_o<P, false>(nt, by, nz)
+                                                       : fold_smem_o<P, true>(nt, by, nz);
+}
+
+}  // namespace
+
+template <class P>
+FoldShape fold_shape(int nz, int ntr) {
+    const FoldTuning t = fold_tuning();
+    FoldShape s{0, 0};
+    if (!(P::kMixed ? t.enable_mixed : t.enable)) return s;
+    const int want_by = t.rows == 1 ? 1 : 2;
+    const int cap_nt = t.tracers > 0 ? t.tracers : 4;
+    // the rows asked for first, then the most tracers per pass that keep two
+    // blocks per SM (one block if nothing else fits), never more than needed
+    for (int pass = 0; pass < 2 && s.nt == 0; ++pass) {
+        const size_t budget = pass == 0 ? kFoldSmemTwo : kFoldSmemMax;
+        for (int by : {want_by, 3 - want_by}) {
+            for (int nt : {4, 2, 1}) {
+                if (nt > cap_nt || (nt > 1 && nt / 2 >= ntr)) continue;
+                if (fold_smem<P>(nt, by, nz) <= budget) {
+                    s.nt = nt;
+                    s.by = by;
+                    break;
+                }
+            }
+            if (s.nt) break;
+        }
+    }
+    return s;
+}
+
 template <class P>
 cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg,
                            cudaStream_t st, Band band) {
     const BandRanges r = band_ranges(rc.nx, rc.ny, band);
+    const FoldShape fs = fold_shape<P>(rc.nz, ff.ntr);
+    if (fs.nt > 0) {
+        if (r.c1 > r.c0) {
+            const int ngroups = (rc.ntr + 1) / 2;
+            const int nb = r.c1 - r.c0;
+            const long long n = (long long)nb * ngroups;
+            const int kid = P::kMixed ? K_MIXED_RECON : K_TRACER_RECON;
+            launch_begin(kid, st);
+            plain::k_tracer_recon<2, P><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc, r.c0, nb);
+            launch_end(kid, st);
+        }
+        if (r.j1 <= r.j0) return cudaGetLastError();
+        fold::FoldArgsT<P> fa{};
+        fa.nx = ff.nx; fa.ny = ff.ny; fa.nz = ff.nz; fa.ntr = ff.ntr;
+        fa.nghost = ff.nghost; fa.nxp = ff.nxp; fa.nyp = ff.nyp;
+        fa.wall_w = ff.wall_w; fa.wall_e = ff.wall_e; fa.wall_s = ff.wall_s; fa.wall_n = ff.wall_n;
+        fa.dt = ff.dt; fa.khtr = ff.khtr; fa.khtr_u = ff.khtr_u; fa.khtr_v = ff.khtr_v;
+        fa.dy_cu = ff.dy_cu; fa.dx_cv = ff.dx_cv; fa.idxCu = ff.idxCu; fa.idyCv = ff.idyCv; fa.areaT = cg.areaT;
+        fa.u = ff.u; fa.v = ff.v; fa.ti = ff.ti; fa.ppm = ff.ppm; fa.err = cg.err;
+        fa.abort = cg.err ? cg.err + 1 : nullptr;  // the word after the error count (both in a scratch header)
+        for (int n = 0; n < ff.ntr; ++n) {
+            fa.htr[n] = cg.htr[n];
+            fa.htr_in[n] = cg.htr_in[n];
+        }
+        if (fs.by == 1) {
+            switch (fs.nt) {
+                case 4: return launch_fold_t<4, P, 1>(fa, r.j0, r.j1, st);
+                case 2: return launch_fold_t<2, P, 1>(fa, r.j0, r.j1, st);
+                default: return launch_fold_t<1, P, 1>(fa, r.j0, r.j1, st);
+            }
+        }
+        switch (fs.nt) {
+            case 4: return launch_fold_t<4, P, 2>(fa, r.j0, r.j1, st);
+            case 2: return launch_fold_t<2, P, 2>(fa, r.j0, r.j1, st);
+            default: return launch_fold_t<1, P, 2>(fa, r.j0, r.j1, st);
+        }
+    }
     // Reconstruct in groups of two tracers (register window of 2 scalars).
     if (r.c1 > r.c0) {
         const int ngroups = (rc.ntr + 1) / 2;
@@ -233,6 +356,8 @@ template cudaError_t launch_sweep<PlainPrec>(const SweepArgsT<PlainPrec>&, cudaS
 template cudaError_t launch_sweep<MixedPrec>(const SweepArgsT<MixedPrec>&, cudaStream_t, Band);
 template cudaError_t launch_phase_b<PlainPrec>(const ReconArgsT<PlainPrec>&, const FaceFluxArgsT<PlainPrec>&,
                                                const CellGatherArgsT<PlainPrec>&, cudaStream_t, Band);
+template FoldShape fold_shape<PlainPrec>(int, int);
+template FoldShape fold_shape<MixedPrec>(int, int);
 template cudaError_t launch_phase_b<MixedPrec>(const ReconArgsT<MixedPrec>&, const FaceFluxArgsT<MixedPrec>&,
                                                const CellGatherArgsT<MixedPrec>&, cudaStream_t, Band);
 

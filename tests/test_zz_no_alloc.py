@@ -97,3 +97,48 @@ def test_noalloc_rejects_domains_beyond_its_scratch():
     assert "limited to 67108608 bytes" in msg, msg
     torch.cuda.synchronize()
     assert torch.equal(st["T"], before)
+
+
+def test_noalloc_allocates_nothing_after_the_first_call():
+    """After the first call on the device, further calls leave the device's free memory unchanged:
+    no cudaMalloc, and no allocator cache growing behind the caller's back."""
+    R, L = _lib()
+    p = inputs.make_problem(44, 36, 15, n_seamounts=4, land_fraction=0.2, seed=405)
+    st = _state(p)
+    stream = torch.cuda.current_stream()
+    assert L.redi_b200_opt_launch_noalloc(*_args(p, st), C.c_void_p(stream.cuda_stream)) == R.OK, R.last_error()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert L.redi_b200_opt_launch_noalloc(*_args(p, st), C.c_void_p(stream.cuda_stream)) == R.OK
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
+def _need_bytes(nx, ny, nz):
+    """The scratch the entry point asks for (the formula of csrc/redi_noalloc.cu)."""
+    r = lambda b: (b + 255) & ~255  # noqa: E731
+    ncol = nx * ny
+    need_a = r(ncol * (nz + 1) * 32) + r(ncol * (nz + 1) * 8)
+    need_b = (r(2 * ncol * (nz + 1) * 8) + r(2 * ncol * nz * 32) + r(2 * (2 * nz + 1) * (nx + 1) * ny * 8)
+              + r(2 * (2 * nz + 1) * nx * (ny + 1) * 8))
+    return max(need_a, need_b)
+
+
+def test_noalloc_near_its_limit_at_75_layers():
+    """The largest square domain that fits at nz = 75 (about 5 800 columns): every output equals
+    redi_opt_launch's, bit for bit, on two calls in a row."""
+    R, L = _lib()
+    limit = (64 << 20) - 256
+    n = max(k for k in range(40, 120) if _need_bytes(k + 4, k + 4, 75) <= limit)
+    assert _need_bytes(n + 4, n + 4, 75) > 0.9 * limit
+    p = inputs.make_problem(n, n, 75, n_seamounts=4, land_fraction=0.2, seed=406)
+    ref, got = _state(p), _state(p)
+    stream = torch.cuda.current_stream()
+    for call in range(2):
+        L.redi_opt_launch(*_args(p, ref))
+        rc = L.redi_b200_opt_launch_noalloc(*_args(p, got), C.c_void_p(stream.cuda_stream))
+        assert rc == R.OK, R.last_error()
+        torch.cuda.synchronize()
+        for k in OUTPUTS:
+            assert torch.equal(got[k], ref[k]), f"call {call + 1}: {k} differs"
