@@ -345,6 +345,13 @@ def run_b200(args, rank, world, local_rank):
     if tiling is not None:
         p = tiling.local_problem(p)
     prec = R.FP64 if args.precision == "fp64" else R.MIXED
+    if args.fold or args.flux_staged:
+        from more_benchmarks_dc_ocean_b200 import autotune
+
+        if args.fold:
+            autotune.set_fold(autotune.FOLD_FP64 | autotune.FOLD_MIXED)
+        if args.flux_staged:
+            autotune.set_flux_staged(True)
     dp = R.to_device(p, dev)
     redi = R.make_redi(dp, prec)
     ex = None
@@ -361,12 +368,15 @@ def run_b200(args, rank, world, local_rank):
         if p.ntr > 2:
             tuning["tracer_group"] = autotune.tune_tracer_group(dp, redi, stream=st)
         if dist is not None:  # every rank uses rank 0's choice
-            t = torch.tensor(list(tuning["best"]) + [autotune.get_tracer_group()], dtype=torch.int64, device=dev)
+            best = tuple(tuning["best"]) + (0,) * (4 - len(tuning["best"]))
+            t = torch.tensor(list(best) + [autotune.get_tracer_group(), autotune.get_gather_tracers()[0]],
+                             dtype=torch.int64, device=dev)
             dist.broadcast(t, 0)
             v = [int(x) for x in t.tolist()]
             autotune.set_tuning(*v[:3])
-            autotune.set_tracer_group(v[3])
-            tuning["best"] = tuple(v[:3])
+            autotune.set_tracer_group(v[4])
+            autotune.set_gather_tracers(v[5], bool(v[3]))
+            tuning["best"] = tuple(v[:4])
     L = R.lib()
     L.redi_b200_launch_count.restype = C.c_ulonglong
     L.redi_b200_launch_count.argtypes = [C.c_int]
@@ -453,6 +463,7 @@ def run_b200(args, rank, world, local_rank):
             "clocks": clk,
             "gpu_launches": int(n1 - n0),
             "tuning": {"cell_update_tile": list(tuning["best"][:2]), "vertical_chunk": tuning["best"][2],
+                       "gather_sums": "shared memory" if len(tuning["best"]) > 3 and tuning["best"][3] else "registers",
                        "tracer_group": tuning.get("tracer_group"),
                        "candidates_ms": tuning["ms"]} if tuning else None,
             "hbm_gbs_per_rank": bstep / (ms_all * 1e-3) / 1e9,
@@ -512,16 +523,23 @@ def _mixed_batched(args, p, dp, st, plain_value: float) -> dict:
     redi = R.make_redi(dq, R.MIXED)
     from more_benchmarks_dc_ocean_b200 import autotune
 
+    saved = (autotune.get_tuning(), autotune.get_gather_tracers())
+    shape = autotune.tune(dq, redi, candidates=[(64, 2, 4, 0), (64, 2, 4, 1), (32, 4, 4, 1), (64, 2, 8, 1),
+                                                  (32, 4, 8, 1)], reps=1, use_cache=False, stream=st)
     group = autotune.tune_tracer_group(dq, redi, stream=st)
     ms = _time_steps(dq, redi, st, warm, steps)
     redi.destroy()
     upd = q.ntr * q.nx_phys * q.ny_phys * q.nz / (ms * 1e-3)
     out["batched_c3"] = {"workload": f"config3: mixed-precision Redi step {q.nx_phys}x{q.ny_phys}x{q.nz}, "
                                      f"{q.ntr} tracers; coefficients once per step, every tracer reconstructed in "
-                                     f"one launch, face fluxes in tracer groups of {group['best']} (autotuned)",
+                                     f"one launch, face fluxes in tracer groups of {group['best'][0]}, gathers of "
+                                     f"{group['best'][1]} tracers (autotuned)",
                          "ms_per_step": ms, "value": upd, "unit": UNIT, "steps": steps, "warmup": warm,
-                         "ratio_vs_plain": upd / plain_value, "tracer_group_ms": group["ms"]}
+                         "ratio_vs_plain": upd / plain_value, "tracer_group_ms": group["ms"],
+                         "gather_shape": list(shape["best"]), "gather_shape_ms": shape["ms"]}
     autotune.set_tracer_group(8)
+    autotune.set_tuning(*saved[0])
+    autotune.set_gather_tracers(saved[1][0], saved[1][1])
     del dq
     torch.cuda.empty_cache()
     return out
@@ -1365,6 +1383,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sub", action="store_true", help="skip the mixed (config 2) and batched (config 3) sub-records")
+    ap.add_argument("--fold", action="store_true",
+                    help="Phase B as the fused face-flux + fold pass instead of the face-flux / cell-gather pair")
+    ap.add_argument("--flux-staged", action="store_true",
+                    help="the face flux with its reconstruction staged through shared memory")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--domains", type=int, default=64, help="config4: number of regional domains")

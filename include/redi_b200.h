@@ -218,6 +218,23 @@ REDI_B200_API int redi_b200_eos_points(const redi_b200_eos* eos, int n, const do
  * at higher occupancy; results do not depend on it. */
 REDI_B200_API int redi_b200_set_tracer_group(int max_group);
 REDI_B200_API int redi_b200_get_tracer_group(void);
+
+/* Tracers one cell-gather launch folds (2 or 4; default 2) and where it keeps
+ * a chunk's per-layer sums (smem != 0, the default: the thread's slots in
+ * shared memory, one load-add-store per flux; 0: registers, a select-add over
+ * the chunk), process-wide (no counterpart in the reference). 4 tracers read
+ * the cell-side Ko half as often; results do not depend on either choice.
+ * get returns n and writes the smem choice if the pointer is non-NULL. */
+REDI_B200_API int redi_b200_set_gather_tracers(int n, int smem);
+REDI_B200_API int redi_b200_get_gather_tracers(int* smem);
+
+/* Face flux with the next sublayer's reconstruction values copied into shared
+ * memory (cp.async) while the current one is evaluated (on != 0), or loaded
+ * when needed (0, the default); process-wide, no counterpart in the reference.
+ * The staged form caps the face-flux tracer group at 2. Results do not depend
+ * on it. */
+REDI_B200_API int redi_b200_set_flux_staged(int on);
+REDI_B200_API int redi_b200_get_flux_staged(void);
 /* Phase B as one fused pass per tile of cells (no counterpart in the
  * reference), process-wide: every face's sublayer fluxes are computed once per
  * tile and added to the cells' tendencies in shared memory, so no flux buffer

@@ -20,6 +20,8 @@ from typing import Iterable, Optional, Sequence, Tuple
 
 TILES: Tuple[Tuple[int, int], ...] = ((32, 4), (64, 2), (128, 1), (32, 2), (32, 1))
 CHUNKS: Tuple[int, ...] = (4, 8, 16)
+# Tiles of 128 threads also run the gather with its per-layer sums in shared memory.
+SMEM_TILES: Tuple[Tuple[int, int], ...] = ((32, 4), (64, 2), (128, 1))
 K_CELL_UPDATE = 3
 
 
@@ -96,6 +98,41 @@ def fold_shape(precision: int, nz: int, ntracers: int) -> Tuple[int, int]:
     return r.value, t.value
 
 
+def set_gather_tracers(n: int, smem: bool = False) -> None:
+    """Tracers one cell-gather launch folds (2 or 4) and whether its per-layer sums live in
+    shared memory (smem) or registers."""
+    from . import ocean_redi as R
+
+    L = R.lib()
+    L.redi_b200_set_gather_tracers.argtypes = [C.c_int, C.c_int]
+    R._check(L.redi_b200_set_gather_tracers(int(n), int(bool(smem))))
+
+
+def set_flux_staged(on: bool) -> None:
+    """Face flux with the next sublayer's reconstruction staged in shared memory (cp.async)."""
+    from . import ocean_redi as R
+
+    L = R.lib()
+    L.redi_b200_set_flux_staged.argtypes = [C.c_int]
+    R._check(L.redi_b200_set_flux_staged(int(bool(on))))
+
+
+def get_flux_staged() -> bool:
+    from . import ocean_redi as R
+
+    return bool(R.lib().redi_b200_get_flux_staged())
+
+
+def get_gather_tracers() -> Tuple[int, bool]:
+    from . import ocean_redi as R
+
+    L = R.lib()
+    L.redi_b200_get_gather_tracers.argtypes = [C.POINTER(C.c_int)]
+    sm = C.c_int()
+    n = L.redi_b200_get_gather_tracers(C.byref(sm))
+    return int(n), bool(sm.value)
+
+
 def get_tracer_group() -> int:
     from . import ocean_redi as R
 
@@ -103,20 +140,22 @@ def get_tracer_group() -> int:
 
 
 def tune_tracer_group(dp, redi, reps: int = 2, stream=None) -> dict:
-    """Time redi_apply_flux for every tracer-group cap the tracer count allows; keep the fastest.
-
-    Advances dp's tracers in place. Returns {"best": cap, "ms": {cap: ms per apply_flux}}.
+    """Time redi_apply_flux for every (face-flux tracer group, tracers per gather) the tracer count
+    allows; keep the fastest. Advances dp's tracers in place. Returns
+    {"best": (group, gather tracers), "ms": {...: ms per apply_flux}}.
     """
     import torch
 
     from . import ocean_redi as R
 
     ntr = len(dp.ms.tracers)
-    caps = [g for g in (2, 4, 8) if g <= max(2, ntr)]
+    smem = get_gather_tracers()[1]
+    caps = [(g, n) for g in (2, 4, 8) if g <= max(2, ntr) for n in (2, 4) if n <= g]
     st = torch.cuda.current_stream() if stream is None else stream
     times = {}
     for g in caps:
-        set_tracer_group(g)
+        set_tracer_group(g[0])
+        set_gather_tracers(g[1], smem)
         R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, st)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
@@ -126,8 +165,9 @@ def tune_tracer_group(dp, redi, reps: int = 2, stream=None) -> dict:
         torch.cuda.synchronize()
         times[g] = e0.elapsed_time(e1) / reps
     best = min(times, key=times.get)
-    set_tracer_group(best)
-    return {"best": best, "ms": {str(g): round(v, 4) for g, v in times.items()}}
+    set_tracer_group(best[0])
+    set_gather_tracers(best[1], smem)
+    return {"best": best, "ms": {f"flux{g}/gather{n}": round(v, 4) for (g, n), v in times.items()}}
 
 
 def _key(dp, precision: int) -> str:
@@ -166,12 +206,19 @@ def _store(dp, precision: int, best) -> None:
         pass
 
 
-def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, int, int]]] = None, reps: int = 2,
-         use_cache: bool = True, stream=None) -> dict:
-    """Time the cell update for every (bx, by, chunk) candidate and keep the fastest.
+def _apply(cand) -> None:
+    """(bx, by, chunk[, smem]) -> the library's gather shape; the tracer count per gather is kept."""
+    set_tuning(*cand[:3])
+    set_gather_tracers(get_gather_tracers()[0], bool(cand[3]) if len(cand) > 3 else False)
 
+
+def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, ...]]] = None, reps: int = 2,
+         use_cache: bool = True, stream=None) -> dict:
+    """Time the cell update for every (bx, by, chunk[, smem]) candidate and keep the fastest.
+
+    smem = 1 runs the gather with its per-layer sums in shared memory (128-thread tiles).
     Runs redi_apply_flux on ``dp`` (its tracers are advanced in place). Returns
-    {"best": (bx, by, chunk), "ms": {candidate: ms per launch}, "cached": bool}.
+    {"best": (bx, by, chunk, smem), "ms": {candidate: ms per launch}, "cached": bool}.
     """
     import torch
 
@@ -181,14 +228,16 @@ def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, int, int]]] = None, 
     if use_cache:
         hit = load_cached(dp, prec)
         if hit:
-            set_tuning(*hit)
+            _apply(hit)
             return {"best": hit, "ms": {}, "cached": True}
     L = _bind(R.lib())
-    cands = list(candidates) if candidates is not None else [(bx, by, c) for (bx, by) in TILES for c in CHUNKS]
+    cands = list(candidates) if candidates is not None else (
+        [(bx, by, c, 0) for (bx, by) in TILES for c in CHUNKS] +
+        [(bx, by, c, 1) for (bx, by) in SMEM_TILES for c in CHUNKS])
     R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, stream)
     times = {}
     for cand in cands:
-        set_tuning(*cand)
+        _apply(cand)
         R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, stream)
         torch.cuda.synchronize()
         L.redi_b200_profile_begin()
@@ -200,9 +249,10 @@ def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, int, int]]] = None, 
         kid = K_CELL_UPDATE
         times[cand] = kt[kid] / max(1, kc[kid])
     best = min(times, key=times.get)
-    set_tuning(*best)
+    _apply(best)
     _store(dp, prec, best)
-    return {"best": best, "ms": {f"{a}x{b}/ch{c}": round(v, 4) for (a, b, c), v in times.items()}, "cached": False}
+    return {"best": best, "ms": {f"{k[0]}x{k[1]}/ch{k[2]}" + ("/smem" if len(k) > 3 and k[3] else ""): round(v, 4)
+                                 for k, v in times.items()}, "cached": False}
 
 
 # Gather tiles of the persistent multi-domain kernel: its blocks are 128 threads.

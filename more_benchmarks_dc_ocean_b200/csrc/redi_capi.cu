@@ -277,7 +277,7 @@ Profiler g_prof;
 namespace redi {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-static CellTuning g_cell_tuning{64, 2, 4, 8};  // the autotuner's usual choice at config 1
+static CellTuning g_cell_tuning{64, 2, 8, 8, 2, 1};  // the autotuner's usual choice at config 1
 CellTuning cell_tuning() { return g_cell_tuning; }
 void set_cell_tuning(const CellTuning& t) { g_cell_tuning = t; }
 static FoldTuning g_fold_tuning{0, 2, 0, 0, 0};  // the pair stays the default until the fused pass is faster
@@ -374,7 +374,11 @@ int redi_b200_set_tuning(int bx, int by, int chunk) {
         return fail(REDI_B200_E_ARG, "redi_b200_set_tuning: bx*by must be a multiple of 32 and at most 128");
     if (chunk != 4 && chunk != 8 && chunk != 16)
         return fail(REDI_B200_E_ARG, "redi_b200_set_tuning: chunk must be 4, 8 or 16");
-    redi::set_cell_tuning(redi::CellTuning{bx, by, chunk, redi::cell_tuning().group});
+    redi::CellTuning t = redi::cell_tuning();
+    t.bx = bx;
+    t.by = by;
+    t.chunk = chunk;
+    redi::set_cell_tuning(t);
     return REDI_B200_OK;
 }
 
@@ -388,6 +392,30 @@ int redi_b200_set_tracer_group(int max_group) {
 }
 
 int redi_b200_get_tracer_group(void) { return redi::cell_tuning().group; }
+
+int redi_b200_set_gather_tracers(int n, int smem) {
+    if (n != 2 && n != 4) return fail(REDI_B200_E_ARG, "redi_b200_set_gather_tracers: n must be 2 or 4");
+    redi::CellTuning t = redi::cell_tuning();
+    t.gather_tracers = n;
+    t.gather_smem = smem ? 1 : 0;
+    redi::set_cell_tuning(t);
+    return REDI_B200_OK;
+}
+
+int redi_b200_set_flux_staged(int on) {
+    redi::CellTuning t = redi::cell_tuning();
+    t.flux_staged = on ? 1 : 0;
+    redi::set_cell_tuning(t);
+    return REDI_B200_OK;
+}
+
+int redi_b200_get_flux_staged(void) { return redi::cell_tuning().flux_staged; }
+
+
+int redi_b200_get_gather_tracers(int* smem) {
+    if (smem) *smem = redi::cell_tuning().gather_smem;
+    return redi::cell_tuning().gather_tracers;
+}
 
 int redi_b200_set_fold(int enable, int rows, int tracers) {
     if (rows != 1 && rows != 2) return fail(REDI_B200_E_ARG, "redi_b200_set_fold: rows must be 1 or 2");

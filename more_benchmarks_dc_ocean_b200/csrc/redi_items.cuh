@@ -746,6 +746,241 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
 }
 
 // ---------------------------------------------------------------------------
+// The face flux with its reconstruction loads staged one sublayer ahead.
+//
+// flux_item waits one memory round trip per sublayer: the reconstruction
+// values a sublayer needs sit at layers given by its own Ko. Here the Ko of
+// the next sublayer is known one iteration early (the coefficients run two
+// surfaces ahead), so its reconstruction values are copied into this thread's
+// slots in shared memory with cp.async while the current sublayer is
+// evaluated from the other slot; the copies hold no registers while in
+// flight. The arithmetic, the values and the stores are exactly flux_item's.
+// Per thread and slot (sublayer parity), structure of arrays so that the
+// threads of a warp touch consecutive words:
+//   ti [slot][tracer][8][kFluxThreads] doubles: bottom-surface interface
+//      values L0, L1, R0, R1, then the top-surface ones (staged only after a
+//      sublayer that the whole warp skipped);
+//   pp [slot][tracer][side][kU][kFluxThreads] 16-byte units: the prepared PPM
+//      layer of the top layer, left then right column.
+// ---------------------------------------------------------------------------
+constexpr int kFluxThreads = 128;
+
+template <class P>
+struct PpmUnits;
+template <>
+struct PpmUnits<PlainPrec> {
+    static constexpr int n = 2;
+};
+template <>
+struct PpmUnits<MixedPrec> {
+    static constexpr int n = 1;
+};
+
+template <int NT, class P>
+struct FluxStage {
+    static constexpr int kU = PpmUnits<P>::n;
+    static constexpr size_t ti_doubles = (size_t)2 * NT * 8 * kFluxThreads;
+    static constexpr size_t pp_units = (size_t)2 * NT * 2 * kU * kFluxThreads;
+    static constexpr size_t bytes = ti_doubles * 8 + pp_units * 16;
+};
+
+template <class P>
+__device__ __forceinline__ typename FluxOps<P>::Raw ld_stage_ppm(const double2* u);
+template <>
+__device__ __forceinline__ PpmLayer ld_stage_ppm<PlainPrec>(const double2* u) {
+    const double2 a = u[0], b = u[kFluxThreads];
+    PpmLayer r;
+    r.aL = a.x; r.dA = a.y; r.a6o3 = b.x; r.B = b.y;
+    return r;
+}
+template <>
+__device__ __forceinline__ float4 ld_stage_ppm<MixedPrec>(const double2* u) {
+    return *reinterpret_cast<const float4*>(u);
+}
+
+template <int NT, class P>
+__device__ __forceinline__ void flux_item_staged(const FaceFluxArgsT<P>& a, int dir, int t, int tr0, int t_end,
+                                                 double* __restrict__ sti, double2* __restrict__ spp) {
+    using Ops = FluxOps<P>;
+    using Raw = typename Ops::Raw;
+    using He = typename P::He;
+    constexpr int kU = PpmUnits<P>::n;
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    const size_t ncol = (size_t)nx * ny;
+    const int tid = threadIdx.x;
+    int colL, colR, fo;
+    size_t fstride;
+    bool valid;
+    if ((dir == 0 ? (nx - 1) * ny : nx * (ny - 1)) <= 0) return;  // no face 0 to stand in
+    if (dir == 0) {
+        valid = t < min(t_end, (nx - 1) * ny);
+        const int tt = valid ? t : 0;
+        const int j = tt / (nx - 1), fi = 1 + tt % (nx - 1);
+        const int I = fi + 1;
+        valid = valid && !((a.wall_w && I == a.nghost + 1) || (a.wall_e && I == a.nghost + a.nxp + 1));
+        colL = (fi - 1) + nx * j;
+        colR = fi + nx * j;
+        fo = fi + (nx + 1) * j;
+        fstride = (size_t)(nx + 1) * ny;
+    } else {
+        valid = t < min(t_end, nx * (ny - 1));
+        const int tt = valid ? t : 0;
+        const int fj = 1 + tt / nx, i = tt % nx;
+        const int J = fj + 1;
+        valid = valid && !((a.wall_s && J == a.nghost + 1) || (a.wall_n && J == a.nghost + a.nyp + 1));
+        colL = i + nx * (fj - 1);
+        colR = i + nx * fj;
+        fo = i + nx * fj;
+        fstride = (size_t)nx * (ny + 1);
+    }
+    if (!__any_sync(0xffffffffu, valid)) return;  // warp-uniform
+    const FaceInT<P>& c = dir == 0 ? a.u : a.v;
+    const He* __restrict__ hEff = c.hEff + fo;
+    const typename P::Po* __restrict__ PoL = c.PoL + fo;
+    const typename P::Po* __restrict__ PoR = c.PoR + fo;
+    const typename P::Ko* __restrict__ KoL = c.KoL + fo;
+    const typename P::Ko* __restrict__ KoR = c.KoR + fo;
+    const double* kh = dir == 0 ? a.khtr_u : a.khtr_v;
+    const double khv = kh ? __ldg(kh + fo) : a.khtr;
+    // ((dt*khtr)*dy)*idx, ocean_redi.F90:1156/1168
+    const double coef = a.dt * khv * __ldg((dir == 0 ? a.dy_cu : a.dx_cv) + fo) *
+                        __ldg((dir == 0 ? a.idxCu : a.idyCv) + fo);
+    const int nt = min(NT, a.ntr - tr0);
+    const size_t ti_stride = ncol * (nz + 1), pp_stride = ncol * nz, f_stride = (size_t)(ns - 1) * fstride;
+    const double* const tiL0 = a.ti + (size_t)tr0 * ti_stride + colL;
+    const double* const tiR0 = a.ti + (size_t)tr0 * ti_stride + colR;
+    const typename P::Ppm* const ppL0 = a.ppm + (size_t)tr0 * pp_stride + colL;
+    const typename P::Ppm* const ppR0 = a.ppm + (size_t)tr0 * pp_stride + colR;
+    typename P::Flux* const Fo0 = (dir == 0 ? a.Fu : a.Fv) + fo;
+    auto trc = [nt](int n) { return (size_t)(n < nt ? n : 0); };
+    auto sti_at = [&](int slot, int n, int w) { return sti + ((size_t)((slot * NT + n) * 8 + w)) * kFluxThreads + tid; };
+    auto spp_at = [&](int slot, int n, int side) {
+        return spp + ((size_t)(((slot * NT + n) * 2 + side) * kU)) * kFluxThreads + tid;
+    };
+    // The staged loads of one sublayer: the bottom surface's interface values
+    // at (klb, krb), the top layer's PPM at (klt, krt) and, if top, the top
+    // surface's interface values.
+    auto issue = [&](int slot, int klt, int krt, int klb, int krb, bool top) {
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            const double* tL = tiL0 + trc(n) * ti_stride;
+            const double* tR = tiR0 + trc(n) * ti_stride;
+            cp_async8(sti_at(slot, n, 0), tL + (size_t)(klb - 1) * ncol);
+            cp_async8(sti_at(slot, n, 1), tL + (size_t)klb * ncol);
+            cp_async8(sti_at(slot, n, 2), tR + (size_t)(krb - 1) * ncol);
+            cp_async8(sti_at(slot, n, 3), tR + (size_t)krb * ncol);
+            if (top) {
+                cp_async8(sti_at(slot, n, 4), tL + (size_t)(klt - 1) * ncol);
+                cp_async8(sti_at(slot, n, 5), tL + (size_t)klt * ncol);
+                cp_async8(sti_at(slot, n, 6), tR + (size_t)(krt - 1) * ncol);
+                cp_async8(sti_at(slot, n, 7), tR + (size_t)krt * ncol);
+            }
+            const char* pL = reinterpret_cast<const char*>(ppL0 + trc(n) * pp_stride + (size_t)(klt - 1) * ncol);
+            const char* pR = reinterpret_cast<const char*>(ppR0 + trc(n) * pp_stride + (size_t)(krt - 1) * ncol);
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                cp_async16(spp_at(slot, n, 0) + (size_t)u * kFluxThreads, pL + 16 * u);
+                cp_async16(spp_at(slot, n, 1) + (size_t)u * kFluxThreads, pR + 16 * u);
+            }
+        }
+    };
+
+    // Coefficients: top surface s, bottom s+1 (hEff(s)), next s+2 (hEff(s+1)),
+    // and s+3 (hEff(s+2)) in flight.
+    int kl_t = min(max((int)__ldg(KoL), 1), nz), kr_t = min(max((int)__ldg(KoR), 1), nz);
+    double pl_t = __ldg(PoL), pr_t = __ldg(PoR);
+    He he_c = __ldg(hEff);
+    int klr_c = __ldg(KoL + fstride), krr_c = __ldg(KoR + fstride);
+    double pl_c = __ldg(PoL + fstride), pr_c = __ldg(PoR + fstride);
+    He he_n = He(0);
+    int klr_n = 1, krr_n = 1;
+    double pl_n = 0.0, pr_n = 0.0;
+    if (ns - 1 > 1) {
+        he_n = __ldg(hEff + fstride);
+        klr_n = __ldg(KoL + 2 * fstride);
+        krr_n = __ldg(KoR + 2 * fstride);
+        pl_n = __ldg(PoL + 2 * fstride);
+        pr_n = __ldg(PoR + 2 * fstride);
+    }
+    bool staged = __any_sync(0xffffffffu, valid && he_c != He(0));  // sublayer 0 staged (warp-uniform)
+    if (staged) issue(0, kl_t, kr_t, min(max(klr_c, 1), nz), min(max(krr_c, 1), nz), true);
+    cp_async_commit();
+    bool have_t = false;  // tl / tr hold the top surface's values (warp-uniform)
+    double tl[NT], tr[NT];
+    for (int s = 0; s < ns - 1; ++s) {
+        const size_t s0 = (size_t)s * fstride;
+        He he_nn = He(0);
+        int klr_nn = 1, krr_nn = 1;
+        double pl_nn = 0.0, pr_nn = 0.0;
+        if (s + 2 < ns - 1) {
+            const size_t s3 = s0 + 3 * fstride;
+            he_nn = __ldg(hEff + s0 + 2 * fstride);
+            klr_nn = __ldg(KoL + s3);
+            krr_nn = __ldg(KoR + s3);
+            pl_nn = __ldg(PoL + s3);
+            pr_nn = __ldg(PoR + s3);
+        }
+        const int kl_b = min(max(klr_c, 1), nz), kr_b = min(max(krr_c, 1), nz);
+        const double pl_b = pl_c, pr_b = pr_c;
+        // the next sublayer's loads: its top surface is this one's bottom
+        bool staged_next = false;
+        if (s + 1 < ns - 1) {
+            staged_next = __any_sync(0xffffffffu, valid && he_n != He(0));
+            if (staged_next)
+                issue((s + 1) & 1, kl_b, kr_b, min(max(klr_n, 1), nz), min(max(krr_n, 1), nz), !staged);
+        }
+        cp_async_commit();
+        const int slot = s & 1;
+        if (staged) {
+            cp_async_wait<1>();  // this sublayer's group (only the next one may still be in flight)
+            const double xRl = pl_b + (double)(kl_b - kl_t);
+            const double xRr = pr_b + (double)(kr_b - kr_t);
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                if (!have_t) {
+                    tl[n] = interp(pl_t, *sti_at(slot, n, 4), *sti_at(slot, n, 5));
+                    tr[n] = interp(pr_t, *sti_at(slot, n, 6), *sti_at(slot, n, 7));
+                }
+                const double bl = interp(pl_b, *sti_at(slot, n, 0), *sti_at(slot, n, 1));
+                const double br = interp(pr_b, *sti_at(slot, n, 2), *sti_at(slot, n, 3));
+                if (valid && n < nt) {
+                    const Raw qL = ld_stage_ppm<P>(spp_at(slot, n, 0));
+                    const Raw qR = ld_stage_ppm<P>(spp_at(slot, n, 1));
+                    const typename Ops::Mean tlay = Ops::mean(pl_t, xRl, qL);
+                    const typename Ops::Mean trlay = Ops::mean(pr_t, xRr, qR);
+                    const double dT = guarded_dT(tr[n] - tl[n], br - bl, (double)(trlay - tlay));
+                    Fo0[(size_t)n * f_stride + s0] = he_c == He(0) ? typename P::Flux(0) : Ops::flux(dT, he_c, coef);
+                }
+                tl[n] = bl;
+                tr[n] = br;
+            }
+            have_t = true;
+        } else {
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+                if (valid && n < nt) Fo0[(size_t)n * f_stride + s0] = typename P::Flux(0);
+            have_t = false;
+        }
+        kl_t = kl_b;
+        kr_t = kr_b;
+        pl_t = pl_b;
+        pr_t = pr_b;
+        he_c = he_n;
+        klr_c = klr_n;
+        krr_c = krr_n;
+        pl_c = pl_n;
+        pr_c = pr_n;
+        he_n = he_nn;
+        klr_n = klr_nn;
+        krr_n = krr_nn;
+        pl_n = pl_nn;
+        pr_n = pr_nn;
+        staged = staged_next;
+    }
+    cp_async_wait<0>();  // nothing may land in the slots after this face is done
+}
+
+// ---------------------------------------------------------------------------
 // Phase B, step 3: per-cell flux divergence (redi_apply_flux_impl,
 // ocean_redi.F90:1094-1181).
 //
@@ -884,6 +1119,118 @@ __device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, 
 #pragma unroll
     for (int f = 0; f < 4; ++f)
         if (on[f] && ptr[f] < ns - 1) ++bad;  // fluxes whose cell-side layer is beyond nz
+    if (bad && a.err) atomicAdd(a.err, bad);
+}
+
+// The same fold with the chunk's per-layer sums of this thread in shared
+// memory (acc: [CH][NT] doubles at a stride of kGatherThreads, this thread's
+// column): each term is one load-add-store at its own layer, so neither the
+// instruction count nor the registers grow with CH x NT. The additions and
+// their order are exactly those of gather_run.
+constexpr int kGatherThreads = 128;
+
+template <int NT, int CH, class P, class LD, int U = 4>
+__device__ __forceinline__ void gather_run_s(const typename P::Flux* const (&F)[NT],
+                                             const typename P::Ko* __restrict__ KoS, size_t stride, bool left, int ns,
+                                             int& ptr, int k0, int k1, double* __restrict__ acc, int& bad) {
+    int s = ptr;
+    while (s < ns - 1) {
+        int kk[U];
+        double ff[U][NT];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int su = s + u;
+            if (su < ns - 1) {
+                const size_t so = (size_t)su * stride;
+                kk[u] = (int)LD::ld(KoS + so);
+#pragma unroll
+                for (int n = 0; n < NT; ++n) ff[u][n] = (double)LD::ld(F[n] + so);
+            } else {
+                kk[u] = 0x7fffffff;
+#pragma unroll
+                for (int n = 0; n < NT; ++n) ff[u][n] = 0.0;
+            }
+        }
+        bool stop = false;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = kk[u];
+            stop = stop || k >= k1;  // also the end of the face (s >= ns-1)
+            if (!stop) {
+                ++s;
+                if (k < k0) {
+                    ++bad;
+                } else {
+                    double* d = acc + (size_t)(k - k0) * NT * kGatherThreads;
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) {
+                        const double v = d[n * kGatherThreads];
+                        d[n * kGatherThreads] = left ? v + ff[u][n] : v - ff[u][n];
+                    }
+                }
+            }
+        }
+        if (stop) break;
+    }
+    ptr = s;
+}
+
+template <int NT, int CH, class P, class LD, int U = 4>
+__device__ __forceinline__ void gather_item_s(const CellGatherArgsT<P>& a, int i, int j, int tr0, int fslot,
+                                              double* __restrict__ acc) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    if (i >= nx || j >= ny) return;
+    const size_t ncol = (size_t)nx * ny;
+    const int col = i + nx * j;
+    const int nt = min(NT, a.ntr - tr0);
+    const int I = i + 1, J = j + 1;  // Fortran indices
+    const int wuf_w = a.nghost + 1, wuf_e = a.nghost + a.nxp + 1;
+    const int wvf_s = a.nghost + 1, wvf_n = a.nghost + a.nyp + 1;
+    const size_t ustride = (size_t)(nx + 1) * ny, vstride = (size_t)nx * (ny + 1);
+    const bool on[4] = {I >= 2 && !((a.wall_w && I == wuf_w) || (a.wall_e && I == wuf_e)),
+                        I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e)),
+                        J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n)),
+                        J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))};
+    const int fo[4] = {i + (nx + 1) * j, i + 1 + (nx + 1) * j, i + nx * j, i + nx * (j + 1)};
+    const double iaij = 1.0 / LD::ld(a.areaT + col);
+    int ptr[4] = {0, 0, 0, 0};
+    int bad = 0;
+    for (int k0 = 1; k0 <= nz; k0 += CH) {
+        const int k1 = min(k0 + CH, nz + 1);
+#pragma unroll
+        for (int x = 0; x < CH * NT; ++x) acc[x * kGatherThreads] = 0.0;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            if (!on[f]) continue;
+            const bool u = f < 2, left = (f & 1) != 0;
+            const size_t stride = u ? ustride : vstride;
+            const typename P::Flux* F[NT];
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+                F[n] = (u ? a.Fu : a.Fv) + (size_t)(fslot + (n < nt ? n : 0)) * (size_t)(ns - 1) * stride + fo[f];
+            const FaceInT<P>& c = u ? a.u : a.v;
+            gather_run_s<NT, CH, P, LD, U>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1, acc,
+                                           bad);
+        }
+        // Layers k0..k1-1 are complete: hTr(knat) += dTr(knat) * (1/areaT), knat = nz + 1 - k.
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            if (n >= nt) break;
+            double* __restrict__ out = a.htr[tr0 + n] + col;
+            const double* __restrict__ in = a.htr_in[tr0 + n] + col;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) {
+                const int k = k0 + c;
+                if (k < k1) {
+                    const size_t o = (size_t)(nz - k) * ncol;
+                    out[o] = in[o] + acc[(c * NT + n) * kGatherThreads] * iaij;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+        if (on[f] && ptr[f] < ns - 1) ++bad;
     if (bad && a.err) atomicAdd(a.err, bad);
 }
 

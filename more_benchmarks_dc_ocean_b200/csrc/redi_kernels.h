@@ -198,9 +198,13 @@ void count_launches(int kid, unsigned long long n);
 
 // Launch shape of Phase B: the cell gather's bx x by tile of columns per
 // block (bx * by <= 128) and vertical chunk (layers per pass, 4, 8 or 16),
-// and the largest tracer group of one face-flux launch (1, 2, 4 or 8).
+// the largest tracer group of one face-flux launch (1, 2, 4 or 8) and the
+// tracers one gather launch folds (2 or 4).
 struct CellTuning {
     int bx, by, chunk, group;
+    int gather_tracers = 2;
+    int gather_smem = 0;  // per-layer sums in shared memory (128-thread tiles) instead of registers
+    int flux_staged = 0;  // face flux with its reconstruction loads staged one sublayer ahead (groups <= 2)
 };
 CellTuning cell_tuning();
 void set_cell_tuning(const CellTuning& t);

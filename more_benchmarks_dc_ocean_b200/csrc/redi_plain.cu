@@ -77,11 +77,35 @@ __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0, 
     flux_item<NT, P, LdNC>(a, d, r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x, tr0, r.hi[d]);
 }
 
+// The face flux with its reconstruction loads staged one sublayer ahead
+// through shared memory (flux_item_staged); the same block order.
+template <int NT, class P>
+__global__ void __launch_bounds__(kFluxThreads) k_face_flux_s(FaceFluxArgsT<P> a, int tr0, FaceRange r) {
+    extern __shared__ __align__(16) unsigned char stage[];
+    double* sti = reinterpret_cast<double*>(stage);
+    double2* spp = reinterpret_cast<double2*>(stage + FluxStage<NT, P>::ti_doubles * sizeof(double));
+    const int d = blockIdx.x & 1;
+    flux_item_staged<NT, P>(a, d, r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x, tr0, r.hi[d], sti,
+                            spp);
+}
+
 template <int NT, int CH, class P>
 __global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgsT<P> a, int tr0, int fslot, int j0, int j1) {
     const int j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
     // sublayers fetched per round trip: 3 with 4-layer chunks, 4 with deeper chunks (measured)
     if (j < j1) gather_item<NT, CH, P, LdNC, (CH <= 4 ? 3 : 4)>(a, blockIdx.x * blockDim.x + threadIdx.x, j, tr0, fslot);
+}
+
+// The gather with its per-layer sums in shared memory (gather_item_s).
+template <int NT, int CH, class P>
+__global__ void __launch_bounds__(kGatherThreads) k_cell_gather_s(CellGatherArgsT<P> a, int tr0, int fslot, int j0,
+                                                                  int j1) {
+    __shared__ double acc[CH * NT * kGatherThreads];
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (j < j1)
+        gather_item_s<NT, CH, P, LdNC, (CH <= 4 ? 3 : 4)>(a, blockIdx.x * blockDim.x + threadIdx.x, j, tr0, fslot,
+                                                          acc + tid);
 }
 
 // The point EOS at n independent points, as the column state evaluates it at
@@ -170,6 +194,30 @@ cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st, Band band) {
     return cudaGetLastError();
 }
 
+template <int GNT, class P>
+static void launch_gather(const CellGatherArgsT<P>& cg, int tr, int slot, const BandRanges& r, const CellTuning& tune,
+                          dim3 cgrid, dim3 block, cudaStream_t st) {
+    launch_begin(K_CELL_UPDATE, st);
+    // shared-memory sums: CH x GNT x 128 doubles must stay within the 48 KB of static shared memory
+    if (tune.gather_smem && block.x * block.y == plain::kGatherThreads && tune.chunk * GNT <= 32) {
+        switch (tune.chunk) {
+            case 4: plain::k_cell_gather_s<GNT, 4, P><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1); break;
+            case 16:
+                if constexpr (GNT <= 2)
+                    plain::k_cell_gather_s<GNT, 16, P><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1);
+                break;
+            default: plain::k_cell_gather_s<GNT, 8, P><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1); break;
+        }
+    } else {
+        switch (tune.chunk) {
+            case 4: plain::k_cell_gather<GNT, 4, P><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1); break;
+            case 16: plain::k_cell_gather<GNT, 16, P><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1); break;
+            default: plain::k_cell_gather<GNT, 8, P><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1); break;
+        }
+    }
+    launch_end(K_CELL_UPDATE, st);
+}
+
 template <int NT, class P>
 static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg, int tr0,
                                const BandRanges& r, const CellTuning& tune, cudaStream_t st) {
@@ -178,29 +226,58 @@ static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT
     const unsigned nb = face_blocks(r.f);
     if (nb > 0) {
         const int kid = P::kMixed ? K_MIXED_FLUX : K_FACE_FLUX;
-        launch_begin(kid, st);
-        plain::k_face_flux<NT, P><<<2 * nb, 128, 0, st>>>(ff, tr0, r.f);
-        launch_end(kid, st);
+        if constexpr (NT <= 2) {
+            if (tune.flux_staged) {
+                // opt into more than 48 KB of dynamic shared memory once per device
+                static int opted[64] = {};
+                int dev = 0;
+                cudaGetDevice(&dev);
+                const int bytes = (int)plain::FluxStage<NT, P>::bytes;
+                if (dev >= 0 && dev < 64 && !opted[dev]) {
+                    cudaFuncSetAttribute(plain::k_face_flux_s<NT, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes);
+                    opted[dev] = 1;
+                }
+                launch_begin(kid, st);
+                plain::k_face_flux_s<NT, P><<<2 * nb, plain::kFluxThreads, bytes, st>>>(ff, tr0, r.f);
+                launch_end(kid, st);
+            } else {
+                launch_begin(kid, st);
+                plain::k_face_flux<NT, P><<<2 * nb, 128, 0, st>>>(ff, tr0, r.f);
+                launch_end(kid, st);
+            }
+        } else {
+            launch_begin(kid, st);
+            plain::k_face_flux<NT, P><<<2 * nb, 128, 0, st>>>(ff, tr0, r.f);
+            launch_end(kid, st);
+        }
     }
     if (cgrid.y == 0) return;
     // The gather folds tracer pairs (its per-layer sums live in registers);
     // a group's pairs read consecutive slots of the flux buffer.
-    for (int g = 0; g < NT; g += 2) {
+    // The gather folds tracer pairs or quads (its per-layer sums live in
+    // registers); a group's tracers read consecutive slots of the flux buffer.
+    const int gnt = (tune.gather_tracers >= 4 && NT >= 4) ? 4 : (NT < 2 ? NT : 2);
+    for (int g = 0; g < NT; g += gnt) {
         if (tr0 + g >= cg.ntr) break;
-        launch_begin(K_CELL_UPDATE, st);
-        switch (tune.chunk) {
-            case 4:
-                plain::k_cell_gather<NT < 2 ? NT : 2, 4, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g, r.j0, r.j1);
-                break;
-            case 16:
-                plain::k_cell_gather<NT < 2 ? NT : 2, 16, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g, r.j0, r.j1);
-                break;
-            default:
-                plain::k_cell_gather<NT < 2 ? NT : 2, 8, P><<<cgrid, block, 0, st>>>(cg, tr0 + g, g, r.j0, r.j1);
-                break;
+        if (gnt == 4) {
+            launch_gather<(NT >= 4 ? 4 : 1), P>(cg, tr0 + g, g, r, tune, cgrid, block, st);
+        } else {
+            launch_gather<(NT < 2 ? NT : 2), P>(cg, tr0 + g, g, r, tune, cgrid, block, st);
         }
-        launch_end(K_CELL_UPDATE, st);
     }
+}
+
+// The tracer reconstruction over the band's columns, two tracers per thread.
+template <class P>
+void launch_recon(const ReconArgsT<P>& rc, const BandRanges& r, cudaStream_t st) {
+    const int ngroups = (rc.ntr + 1) / 2;
+    const int nb = r.c1 - r.c0;
+    const long long n = (long long)nb * ngroups;
+    const int kid = P::kMixed ? K_MIXED_RECON : K_TRACER_RECON;
+    launch_begin(kid, st);
+    plain::k_tracer_recon<2, P><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc, r.c0, nb);
+    launch_end(kid, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -295,13 +372,7 @@ cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, 
     const FoldShape fs = fold_shape<P>(rc.nz, ff.ntr);
     if (fs.nt > 0) {
         if (r.c1 > r.c0) {
-            const int ngroups = (rc.ntr + 1) / 2;
-            const int nb = r.c1 - r.c0;
-            const long long n = (long long)nb * ngroups;
-            const int kid = P::kMixed ? K_MIXED_RECON : K_TRACER_RECON;
-            launch_begin(kid, st);
-            plain::k_tracer_recon<2, P><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc, r.c0, nb);
-            launch_end(kid, st);
+            launch_recon<P>(rc, r, st);
         }
         if (r.j1 <= r.j0) return cudaGetLastError();
         fold::FoldArgsT<P> fa{};
@@ -331,16 +402,11 @@ cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, 
     }
     // Reconstruct in groups of two tracers (register window of 2 scalars).
     if (r.c1 > r.c0) {
-        const int ngroups = (rc.ntr + 1) / 2;
-        const int nb = r.c1 - r.c0;
-        const long long n = (long long)nb * ngroups;
-        const int kid = P::kMixed ? K_MIXED_RECON : K_TRACER_RECON;
-        launch_begin(kid, st);
-        plain::k_tracer_recon<2, P><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rc, r.c0, nb);
-        launch_end(kid, st);
+        launch_recon<P>(rc, r, st);
     }
     const CellTuning tune = cell_tuning();
-    const int group = tracer_group(ff.ntr, tune.group);
+    // the staged face flux holds one or two tracers' reconstruction in shared memory
+    const int group = tracer_group(ff.ntr, tune.flux_staged ? (tune.group < 2 ? tune.group : 2) : tune.group);
     for (int tr0 = 0; tr0 < ff.ntr; tr0 += group) {
         switch (group) {
             case 8: launch_flux_gather<8, P>(ff, cg, tr0, r, tune, st); break;

@@ -279,3 +279,63 @@ def test_mixed_precision_many_tracers_and_gates(redi_lib, oracle_lib):
         # passive tracers cross zero, so compare against each field's scale
         scale = np.abs(ref[n]).max()
         assert np.abs(got[n] - ref[n]).max() <= 1e-7 * scale, n
+
+
+@pytest.mark.parametrize("gnt,smem,chunk", [(2, True, 4), (2, True, 8), (2, True, 16), (4, False, 4), (4, True, 8)])
+def test_gather_forms_match_oracle(redi_lib, oracle_lib, gnt, smem, chunk):
+    """The gather folding 2 or 4 tracers per launch, with its per-layer sums in registers or in
+    shared memory: the same additions in the same order, so the oracle's bits."""
+    from more_benchmarks_dc_ocean_b200 import autotune
+
+    saved = (autotune.get_tuning(), autotune.get_gather_tracers(), autotune.get_tracer_group())
+    try:
+        autotune.set_tuning(64, 2, chunk)
+        autotune.set_gather_tracers(gnt, smem)
+        autotune.set_tracer_group(4)
+        p = inputs.make_problem(45, 27, 19, n_passive=5, seed=23)
+        _, tg = _run_gpu(p, 1, redi_lib, check_coeffs=False)
+        _, to = _run_oracle(p, 1)
+        for n, (a, b) in enumerate(zip(tg, to)):
+            _assert_exact(f"gather gnt={gnt} smem={smem} chunk={chunk} tracer {n}", a, b)
+    finally:
+        autotune.set_tuning(*saved[0])
+        autotune.set_gather_tracers(*saved[1])
+        autotune.set_tracer_group(saved[2])
+
+
+@pytest.mark.parametrize("group,precision", [(1, 0), (2, 0), (2, 1)])
+def test_staged_face_flux_matches(redi_lib, oracle_lib, group, precision):
+    """The face flux with its reconstruction staged through shared memory one sublayer ahead:
+    FP64 equals the oracle bit for bit; the mixed form equals the unstaged mixed form bit for bit."""
+    from more_benchmarks_dc_ocean_b200 import autotune
+
+    R = redi_lib
+    saved = (autotune.get_flux_staged(), autotune.get_tracer_group())
+    p = inputs.make_problem(43, 29, 17, n_passive=3, seed=61)
+    try:
+        autotune.set_tracer_group(group)
+        if precision:
+            autotune.set_flux_staged(False)
+            dp = R.to_device(p)
+            redi = R.make_redi(dp, R.MIXED)
+            R.step(dp, redi, 1)
+            torch.cuda.synchronize()
+            ref = [t.cpu().numpy() for t in dp.ms.tracers]
+            redi.destroy()
+            autotune.set_flux_staged(True)
+            dp = R.to_device(p)
+            redi = R.make_redi(dp, R.MIXED)
+            R.step(dp, redi, 1)
+            torch.cuda.synchronize()
+            got = [t.cpu().numpy() for t in dp.ms.tracers]
+            assert redi.error_count() == 0
+            redi.destroy()
+        else:
+            autotune.set_flux_staged(True)
+            _, got = _run_gpu(p, 1, redi_lib, check_coeffs=False)
+            _, ref = _run_oracle(p, 1)
+        for n, (a, b) in enumerate(zip(got, ref)):
+            _assert_exact(f"staged flux group={group} precision={precision} tracer {n}", a, b)
+    finally:
+        autotune.set_flux_staged(saved[0])
+        autotune.set_tracer_group(saved[1])
