@@ -320,6 +320,15 @@ REDI_B200_API int redi_b200_opt_launch_noalloc(
     const double* dx_cv, const double* idxCu, const double* idyCv, const double* areaT, double* tr_snap,
     void* stream);
 
+/* Halo packing for a domain split into tiles (no counterpart in the reference,
+ * which steps one undivided domain): copies column `index` (axis 0) or row
+ * `index` (axis 1) of each of the nfields (nx, ny, nz) fields (device
+ * pointers; at most 65) into the device buffer buf (to_buf != 0), field after
+ * field, nz x ny or nz x nx values each, layer-major; or from buf back into the
+ * fields (to_buf == 0). One launch, stream-ordered. */
+REDI_B200_API int redi_b200_halo_copy(double* const* fields, int nfields, int nx, int ny, int nz, int axis, int index,
+                                      double* buf, int to_buf, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Many independent regional domains stepped by one persistent kernel (no
  * counterpart in the reference, whose driver steps one domain per call). The

@@ -26,6 +26,7 @@ SOURCES = [
     ("redi_plain.cu", ["-fmad=false"]),
     ("redi_capi.cu", []),
     ("redi_noalloc.cu", []),
+    ("redi_halo.cu", []),
     ("redi_domains.cu", ["-fmad=false"]),
     ("meke.cu", ["-fmad=false"]),
     ("ale.cu", ["-fmad=false"]),

@@ -13,6 +13,9 @@ Exchange: torch.distributed point-to-point (`batch_isend_irecv`), NCCL over
 NVLink/NVSwitch on GPUs, gloo on CPU (tests). Each side packs its first/last
 physical column (or row) of every field, (nz, ny) or (nz, nx) doubles, into one
 contiguous buffer per neighbour; the receiver writes it into its ghost column.
+On the GPU one library launch (`redi_b200_halo_copy`) packs all fields for a
+neighbour and one unpacks them; CPU tensors (the gloo tests) are copied slice by
+slice.
 """
 
 from __future__ import annotations
@@ -138,39 +141,62 @@ class HaloExchange:
         mk = lambda n: torch.empty(n, dtype=fields[0].dtype, device=dev)  # noqa: E731
         self.sides = []
         g = self.g
-        # (neighbour rank, send slice, recv slice, buffer length)
+        # (neighbour rank, send slice, recv slice, send buffer, recv buffer, values per field,
+        #  (axis, send index, recv index) for the library's pack / unpack)
         for dx, dy in ((-1, 0), (1, 0), (0, -1), (0, 1)):
             nb = tiling.neighbour(dx, dy)
             if nb is None:
                 continue
             if dx == -1:
                 send, recv = (slice(None), slice(None), g), (slice(None), slice(None), g - 1)
-                n = nz * ny
+                n, lib = nz * ny, (0, g, g - 1)
             elif dx == 1:
                 send, recv = (slice(None), slice(None), nx - g - 1), (slice(None), slice(None), nx - g)
-                n = nz * ny
+                n, lib = nz * ny, (0, nx - g - 1, nx - g)
             elif dy == -1:
                 send, recv = (slice(None), g, slice(None)), (slice(None), g - 1, slice(None))
-                n = nz * nx
+                n, lib = nz * nx, (1, g, g - 1)
             else:
                 send, recv = (slice(None), ny - g - 1, slice(None)), (slice(None), ny - g, slice(None))
-                n = nz * nx
-            self.sides.append((nb, send, recv, mk(n * nf), mk(n * nf), n))
+                n, lib = nz * nx, (1, ny - g - 1, ny - g)
+            self.sides.append((nb, send, recv, mk(n * nf), mk(n * nf), n, lib))
+
+    def _lib_copy(self, fields, axis: int, index: int, buf, to_buf: bool) -> None:
+        import ctypes as C
+
+        import torch
+
+        from . import ocean_redi as R
+
+        L = R.lib()
+        L.redi_b200_halo_copy.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+        nz, ny, nx = fields[0].shape
+        ptrs = (C.c_void_p * len(fields))(*[t.data_ptr() for t in fields])
+        R._check(L.redi_b200_halo_copy(ptrs, len(fields), nx, ny, nz, axis, index, buf.data_ptr(), int(to_buf),
+                                       torch.cuda.current_stream().cuda_stream))
 
     def exchange(self, fields=None):
         fields = self.fields if fields is None else fields
+        on_gpu = fields[0].is_cuda and all(t.is_contiguous() and t.dtype == fields[0].dtype for t in fields)
         ops = []
-        for nb, send, recv, sbuf, rbuf, n in self.sides:
-            for f, t in enumerate(fields):
-                sbuf[f * n:(f + 1) * n].view(t[send].shape).copy_(t[send])
+        for nb, send, recv, sbuf, rbuf, n, lib in self.sides:
+            if on_gpu:
+                self._lib_copy(fields, lib[0], lib[1], sbuf, True)
+            else:
+                for f, t in enumerate(fields):
+                    sbuf[f * n:(f + 1) * n].view(t[send].shape).copy_(t[send])
             ops.append(self.dist.P2POp(self.dist.isend, sbuf, nb, self.group))
             ops.append(self.dist.P2POp(self.dist.irecv, rbuf, nb, self.group))
         if ops:
             for r in self.dist.batch_isend_irecv(ops):
                 r.wait()
-        for nb, send, recv, sbuf, rbuf, n in self.sides:
-            for f, t in enumerate(fields):
-                t[recv].copy_(rbuf[f * n:(f + 1) * n].view(t[recv].shape))
+        for nb, send, recv, sbuf, rbuf, n, lib in self.sides:
+            if on_gpu:
+                self._lib_copy(fields, lib[0], lib[2], rbuf, False)
+            else:
+                for f, t in enumerate(fields):
+                    t[recv].copy_(rbuf[f * n:(f + 1) * n].view(t[recv].shape))
 
     def setup_masks(self, dp, cell_wet) -> None:
         """Make the face masks on tile edges agree between neighbours.
@@ -204,10 +230,10 @@ class HaloExchange:
         saved = self.sides
         nz = fields[0].shape[0]
         sides = []
-        for nb, send, recv, sbuf, rbuf, n in saved:
+        for nb, send, recv, sbuf, rbuf, n, lib in saved:
             m = n // self.shape[0] * nz
             mk = lambda: torch.empty(m * len(fields), dtype=fields[0].dtype, device=fields[0].device)  # noqa: E731
-            sides.append((nb, send, recv, mk(), mk(), m))
+            sides.append((nb, send, recv, mk(), mk(), m, lib))
         self.sides = sides
         try:
             self.exchange(fields)
