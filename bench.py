@@ -375,7 +375,7 @@ def run_b200(args, rank, world, local_rank):
             v = [int(x) for x in t.tolist()]
             autotune.set_tuning(*v[:3])
             autotune.set_tracer_group(v[4])
-            autotune.set_gather_tracers(v[5], bool(v[3]))
+            autotune.set_gather_tracers(v[5], v[3])
             tuning["best"] = tuple(v[:4])
     L = R.lib()
     L.redi_b200_launch_count.restype = C.c_ulonglong
@@ -463,7 +463,8 @@ def run_b200(args, rank, world, local_rank):
             "clocks": clk,
             "gpu_launches": int(n1 - n0),
             "tuning": {"cell_update_tile": list(tuning["best"][:2]), "vertical_chunk": tuning["best"][2],
-                       "gather_sums": "shared memory" if len(tuning["best"]) > 3 and tuning["best"][3] else "registers",
+                       "gather_sums": {0: "registers", 1: "shared memory", 2: "shared memory, 8-deep batches"}[
+                           tuning["best"][3] if len(tuning["best"]) > 3 else 0],
                        "tracer_group": tuning.get("tracer_group"),
                        "candidates_ms": tuning["ms"]} if tuning else None,
             "hbm_gbs_per_rank": bstep / (ms_all * 1e-3) / 1e9,
@@ -508,24 +509,30 @@ def _mixed_batched(args, p, dp, st, plain_value: float) -> dict:
     from more_benchmarks_dc_ocean_b200 import inputs
     from more_benchmarks_dc_ocean_b200 import ocean_redi as R
 
+    from more_benchmarks_dc_ocean_b200 import autotune
+
     out = {}
     steps, warm = max(3, min(args.steps, 10)), 3
+    saved = (autotune.get_tuning(), autotune.get_gather_tracers())
     redi = R.make_redi(dp, R.MIXED)
+    # The FP64 line's gather shape is not the mixed one's best (FP32 fluxes halve the gather's
+    # loads), so the mixed step picks its own among the shapes that win in either precision.
+    shape2 = autotune.tune(dp, redi, candidates=[(64, 2, 4, 1), (64, 2, 8, 1), (32, 4, 8, 1), (32, 4, 16, 2),
+                                                   (64, 2, 16, 2)], reps=1, use_cache=False, stream=st)
     ms = _time_steps(dp, redi, st, warm, steps)
     redi.destroy()
     upd = p.ntr * p.nx_phys * p.ny_phys * p.nz / (ms * 1e-3)
     out["mixed_c2"] = {"workload": f"config2: mixed-precision Redi step {p.nx_phys}x{p.ny_phys}x{p.nz}, "
                                    f"{p.ntr} tracers (the inputs of this line)",
                        "ms_per_step": ms, "value": upd, "unit": UNIT, "steps": steps, "warmup": warm,
-                       "ratio_vs_plain": upd / plain_value}
+                       "ratio_vs_plain": upd / plain_value, "gather_shape": list(shape2["best"]),
+                       "gather_shape_ms": shape2["ms"]}
     q = inputs.config3()
     dq = R.to_device(q, torch.device("cuda", torch.cuda.current_device()))
     redi = R.make_redi(dq, R.MIXED)
-    from more_benchmarks_dc_ocean_b200 import autotune
-
-    saved = (autotune.get_tuning(), autotune.get_gather_tracers())
     shape = autotune.tune(dq, redi, candidates=[(64, 2, 4, 0), (64, 2, 4, 1), (32, 4, 4, 1), (64, 2, 8, 1),
-                                                  (32, 4, 8, 1)], reps=1, use_cache=False, stream=st)
+                                                  (32, 4, 8, 1), (32, 4, 4, 2), (32, 4, 8, 2)], reps=1,
+                          use_cache=False, stream=st)
     group = autotune.tune_tracer_group(dq, redi, stream=st)
     ms = _time_steps(dq, redi, st, warm, steps)
     redi.destroy()

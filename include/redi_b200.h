@@ -220,8 +220,9 @@ REDI_B200_API int redi_b200_set_tracer_group(int max_group);
 REDI_B200_API int redi_b200_get_tracer_group(void);
 
 /* Tracers one cell-gather launch folds (2 or 4; default 2) and where it keeps
- * a chunk's per-layer sums (smem != 0, the default: the thread's slots in
- * shared memory, one load-add-store per flux; 0: registers, a select-add over
+ * a chunk's per-layer sums (smem = 1, the default: the thread's slots in
+ * shared memory, one load-add-store per flux; 2: the same, fetching 8
+ * sublayers per round trip instead of 3 or 4; 0: registers, a select-add over
  * the chunk), process-wide (no counterpart in the reference). 4 tracers read
  * the cell-side Ko half as often; results do not depend on either choice.
  * get returns n and writes the smem choice if the pointer is non-NULL. */

@@ -98,14 +98,14 @@ def fold_shape(precision: int, nz: int, ntracers: int) -> Tuple[int, int]:
     return r.value, t.value
 
 
-def set_gather_tracers(n: int, smem: bool = False) -> None:
-    """Tracers one cell-gather launch folds (2 or 4) and whether its per-layer sums live in
-    shared memory (smem) or registers."""
+def set_gather_tracers(n: int, smem: int = 0) -> None:
+    """Tracers one cell-gather launch folds (2 or 4) and where its per-layer sums live: 0 registers,
+    1 shared memory, 2 shared memory with 8 sublayers fetched per round trip."""
     from . import ocean_redi as R
 
     L = R.lib()
     L.redi_b200_set_gather_tracers.argtypes = [C.c_int, C.c_int]
-    R._check(L.redi_b200_set_gather_tracers(int(n), int(bool(smem))))
+    R._check(L.redi_b200_set_gather_tracers(int(n), int(smem)))
 
 
 def set_flux_staged(on: bool) -> None:
@@ -123,14 +123,15 @@ def get_flux_staged() -> bool:
     return bool(R.lib().redi_b200_get_flux_staged())
 
 
-def get_gather_tracers() -> Tuple[int, bool]:
+def get_gather_tracers() -> Tuple[int, int]:
+    """(tracers per gather, sums: 0 registers, 1 shared memory, 2 shared memory with 8-deep batches)."""
     from . import ocean_redi as R
 
     L = R.lib()
     L.redi_b200_get_gather_tracers.argtypes = [C.POINTER(C.c_int)]
     sm = C.c_int()
     n = L.redi_b200_get_gather_tracers(C.byref(sm))
-    return int(n), bool(sm.value)
+    return int(n), int(sm.value)
 
 
 def get_tracer_group() -> int:
@@ -209,14 +210,15 @@ def _store(dp, precision: int, best) -> None:
 def _apply(cand) -> None:
     """(bx, by, chunk[, smem]) -> the library's gather shape; the tracer count per gather is kept."""
     set_tuning(*cand[:3])
-    set_gather_tracers(get_gather_tracers()[0], bool(cand[3]) if len(cand) > 3 else False)
+    set_gather_tracers(get_gather_tracers()[0], int(cand[3]) if len(cand) > 3 else 0)
 
 
 def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, ...]]] = None, reps: int = 2,
          use_cache: bool = True, stream=None) -> dict:
     """Time the cell update for every (bx, by, chunk[, smem]) candidate and keep the fastest.
 
-    smem = 1 runs the gather with its per-layer sums in shared memory (128-thread tiles).
+    smem = 1 runs the gather with its per-layer sums in shared memory (128-thread tiles), 2 the same
+    with 8 sublayers fetched per round trip.
     Runs redi_apply_flux on ``dp`` (its tracers are advanced in place). Returns
     {"best": (bx, by, chunk, smem), "ms": {candidate: ms per launch}, "cached": bool}.
     """
@@ -233,7 +235,7 @@ def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, ...]]] = None, reps:
     L = _bind(R.lib())
     cands = list(candidates) if candidates is not None else (
         [(bx, by, c, 0) for (bx, by) in TILES for c in CHUNKS] +
-        [(bx, by, c, 1) for (bx, by) in SMEM_TILES for c in CHUNKS])
+        [(bx, by, c, m) for (bx, by) in SMEM_TILES for c in CHUNKS for m in (1, 2)])
     R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, stream)
     times = {}
     for cand in cands:
@@ -251,7 +253,7 @@ def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, ...]]] = None, reps:
     best = min(times, key=times.get)
     _apply(best)
     _store(dp, prec, best)
-    return {"best": best, "ms": {f"{k[0]}x{k[1]}/ch{k[2]}" + ("/smem" if len(k) > 3 and k[3] else ""): round(v, 4)
+    return {"best": best, "ms": {f"{k[0]}x{k[1]}/ch{k[2]}" + ({1: "/smem", 2: "/smem/u8"}.get(k[3], "") if len(k) > 3 else ""): round(v, 4)
                                  for k, v in times.items()}, "cached": False}
 
 

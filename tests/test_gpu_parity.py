@@ -281,7 +281,8 @@ def test_mixed_precision_many_tracers_and_gates(redi_lib, oracle_lib):
         assert np.abs(got[n] - ref[n]).max() <= 1e-7 * scale, n
 
 
-@pytest.mark.parametrize("gnt,smem,chunk", [(2, True, 4), (2, True, 8), (2, True, 16), (4, False, 4), (4, True, 8)])
+@pytest.mark.parametrize("gnt,smem,chunk", [(2, 1, 4), (2, 1, 8), (2, 1, 16), (4, 0, 4), (4, 1, 8), (2, 2, 8),
+                                            (2, 2, 16), (4, 2, 4)])
 def test_gather_forms_match_oracle(redi_lib, oracle_lib, gnt, smem, chunk):
     """The gather folding 2 or 4 tracers per launch, with its per-layer sums in registers or in
     shared memory: the same additions in the same order, so the oracle's bits."""
