@@ -229,13 +229,22 @@ REDI_B200_API int redi_b200_get_tracer_group(void);
 REDI_B200_API int redi_b200_set_gather_tracers(int n, int smem);
 REDI_B200_API int redi_b200_get_gather_tracers(int* smem);
 
-/* Face flux with the next sublayer's reconstruction values copied into shared
- * memory (cp.async) while the current one is evaluated (on != 0), or loaded
- * when needed (0, the default); process-wide, no counterpart in the reference.
- * The staged form caps the face-flux tracer group at 2. Results do not depend
- * on it. */
+/* Face flux form, process-wide (no counterpart in the reference): 0 loads each
+ * sublayer's reconstruction values when needed; 1 copies the next sublayer's
+ * into shared memory (cp.async) while the current one is evaluated (caps the
+ * face-flux tracer group at 2); 2 reads each column's reconstruction through a
+ * two-layer ring in shared memory, the layer below fetched when a side enters a
+ * layer (caps the group at 4). Results do not depend on it. */
 REDI_B200_API int redi_b200_set_flux_staged(int on);
 REDI_B200_API int redi_b200_get_flux_staged(void);
+/* Neutral sweep form, process-wide (no counterpart in the reference): 0 keeps
+ * each column's three-interface window in registers with a shared-memory
+ * look-ahead ring; 3, 4 (the default) or 5 keeps both windows in a per-thread
+ * shared-memory ring of 3, 4 or 5 interfaces (none, one or two in flight), read
+ * through one code path whichever column the step advances. Results do not
+ * depend on it. */
+REDI_B200_API int redi_b200_set_sweep_form(int form);
+REDI_B200_API int redi_b200_get_sweep_form(void);
 /* Phase B as one fused pass per tile of cells (no counterpart in the
  * reference), process-wide: every face's sublayer fluxes are computed once per
  * tile and added to the cells' tendencies in shared memory, so no flux buffer

@@ -108,19 +108,35 @@ def set_gather_tracers(n: int, smem: int = 0) -> None:
     R._check(L.redi_b200_set_gather_tracers(int(n), int(smem)))
 
 
-def set_flux_staged(on: bool) -> None:
-    """Face flux with the next sublayer's reconstruction staged in shared memory (cp.async)."""
+def set_sweep_form(form: int) -> None:
+    """Neutral sweep form: 0 register windows, 3 / 4 / 5 both windows in a shared-memory ring of that size."""
+    from . import ocean_redi as R
+
+    L = R.lib()
+    L.redi_b200_set_sweep_form.argtypes = [C.c_int]
+    R._check(L.redi_b200_set_sweep_form(int(form)))
+
+
+def get_sweep_form() -> int:
+    from . import ocean_redi as R
+
+    return int(R.lib().redi_b200_get_sweep_form())
+
+
+def set_flux_staged(form: int) -> None:
+    """Face flux form: 0 direct loads, 1 the next sublayer's reconstruction staged in shared memory
+    (cp.async), 2 each column's reconstruction read through a two-layer ring in shared memory."""
     from . import ocean_redi as R
 
     L = R.lib()
     L.redi_b200_set_flux_staged.argtypes = [C.c_int]
-    R._check(L.redi_b200_set_flux_staged(int(bool(on))))
+    R._check(L.redi_b200_set_flux_staged(int(form)))
 
 
-def get_flux_staged() -> bool:
+def get_flux_staged() -> int:
     from . import ocean_redi as R
 
-    return bool(R.lib().redi_b200_get_flux_staged())
+    return int(R.lib().redi_b200_get_flux_staged())
 
 
 def get_gather_tracers() -> Tuple[int, int]:

@@ -277,7 +277,9 @@ Profiler g_prof;
 namespace redi {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-static CellTuning g_cell_tuning{64, 2, 8, 8, 2, 1};  // the autotuner's usual choice at config 1
+// the autotuner's usual gather choice at config 1; the sweep's windows in a
+// shared-memory ring of 4 interfaces
+static CellTuning g_cell_tuning{64, 2, 8, 8, 2, 1, 0, 0, 4};
 CellTuning cell_tuning() { return g_cell_tuning; }
 void set_cell_tuning(const CellTuning& t) { g_cell_tuning = t; }
 static FoldTuning g_fold_tuning{0, 2, 0, 0, 0};  // the pair stays the default until the fused pass is faster
@@ -405,13 +407,25 @@ int redi_b200_set_gather_tracers(int n, int smem) {
 }
 
 int redi_b200_set_flux_staged(int on) {
+    if (on < 0 || on > 2) return fail(REDI_B200_E_ARG, "redi_b200_set_flux_staged: on must be 0, 1 or 2");
     redi::CellTuning t = redi::cell_tuning();
-    t.flux_staged = on ? 1 : 0;
+    t.flux_staged = on;
     redi::set_cell_tuning(t);
     return REDI_B200_OK;
 }
 
 int redi_b200_get_flux_staged(void) { return redi::cell_tuning().flux_staged; }
+
+int redi_b200_set_sweep_form(int form) {
+    if (form != 0 && (form < 3 || form > 5))
+        return fail(REDI_B200_E_ARG, "redi_b200_set_sweep_form: form must be 0, 3, 4 or 5");
+    redi::CellTuning t = redi::cell_tuning();
+    t.sweep_form = form;
+    redi::set_cell_tuning(t);
+    return REDI_B200_OK;
+}
+
+int redi_b200_get_sweep_form(void) { return redi::cell_tuning().sweep_form; }
 
 
 int redi_b200_get_gather_tracers(int* smem) {

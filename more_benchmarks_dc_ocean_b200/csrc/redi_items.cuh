@@ -184,6 +184,11 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
 }
+// L1-allocating 16-byte copy (a warp's left and right columns overlap)
+__device__ __forceinline__ void cp_async16_ca(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
@@ -459,6 +464,235 @@ __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int 
         absR_prev = absR;
     }
     if constexpr (STAGED) cp_async_wait<0>();  // no copy may land in the ring after this face is done
+}
+
+// ---------------------------------------------------------------------------
+// The same sweep with both columns' windows held in a per-thread ring in
+// shared memory instead of registers (the standalone sweep kernel's default).
+//
+// Slot q % NR of side s holds interface min(q, nk) (0-based) of that column.
+// A column with pointer k (1-based) reads interfaces max(k-2, 0) ..
+// max(k-2, 0) + 2: its own interface is always k-1, the reference's km1 is
+// max(k-2, 0). Both columns are read through the same index arithmetic, so the
+// anchor's advance is one code path whichever column it is (the register form
+// duplicates it per column, and a warp whose lanes search in different
+// directions runs both copies). NR = 5 keeps two interfaces in flight per
+// column (fetched two advances before they are read, wait_group 1); NR = 4
+// keeps one (wait_group 0 at each advance); NR = 3 fetches the entering
+// interface at the advance and waits for it at the top of the next step
+// (the smallest ring: more resident blocks, one round trip per advance).
+//
+// The bottom density difference of a searched column with k >= 2 is the step's
+// own dRho with its sign set by the direction: rho(S_k) - rho(A_k) and
+// rho(A_k) - rho(S_k) are exact negatives (a commuted sum, an exactly negated
+// difference, an exactly negated product), and the sign of a zero never
+// reaches a decision (every use compares with 0 or forms a difference with a
+// non-zero value).
+// ---------------------------------------------------------------------------
+template <int NR>
+struct SweepWin {
+    double2 ts[NR][2][kSweepThreads];  // (T, S)
+    double2 dd[NR][2][kSweepThreads];  // (dR/dT, dR/dS)
+    double p[NR][2][kSweepThreads];    // pressure
+};
+
+template <int NR>
+__device__ __forceinline__ void sw_fetch(SweepWin<NR>& r, int side, int q, const IfcState* X, const double* P, int nk,
+                                         size_t ld) {
+    const int slot = q % NR, qi = min(q, nk), tid = threadIdx.x;
+    const double2* src = reinterpret_cast<const double2*>(X + (size_t)qi * ld);
+    cp_async16(&r.ts[slot][side][tid], src);
+    cp_async16(&r.dd[slot][side][tid], src + 1);
+    cp_async8(&r.p[slot][side][tid], P + (size_t)qi * ld);
+}
+
+template <int NR>
+__device__ __forceinline__ IfcState sw_ifc(const SweepWin<NR>& r, int side, int q) {
+    const int slot = q % NR, tid = threadIdx.x;
+    const double2 a = r.ts[slot][side][tid], b = r.dd[slot][side][tid];
+    IfcState s;
+    s.T = a.x;
+    s.S = a.y;
+    s.dRdT = b.x;
+    s.dRdS = b.y;
+    return s;
+}
+
+template <int NR>
+__device__ __forceinline__ double sw_p(const SweepWin<NR>& r, int side, int q) {
+    return r.p[q % NR][side][threadIdx.x];
+}
+
+// r: this block's ring (dynamic shared memory, blocks of kSweepThreads).
+template <class P, class LD, int NR>
+__device__ __forceinline__ void sweep_item_win(const SweepArgsT<P>& a, int dir, int t, SweepWin<NR>& r) {
+    static_assert(NR >= 3 && NR <= 5, "ring of 3 (none in flight), 4 (one) or 5 (two)");
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    const size_t ld = (size_t)nx * ny;
+    int colL, colR, fo;
+    size_t fstride;
+    if (dir == 0) {
+        if (t >= (nx - 1) * ny) return;
+        const int j = t / (nx - 1), fi = 1 + t % (nx - 1);
+        colL = (fi - 1) + nx * j;
+        colR = fi + nx * j;
+        fo = fi + (nx + 1) * j;
+        fstride = (size_t)(nx + 1) * ny;
+    } else {
+        if (t >= nx * (ny - 1)) return;
+        const int fj = 1 + t / nx, i = t % nx;
+        colL = i + nx * (fj - 1);
+        colR = i + nx * fj;
+        fo = i + nx * fj;
+        fstride = (size_t)nx * (ny + 1);
+    }
+    using Po = typename P::Po;
+    using Ko = typename P::Ko;
+    using He = typename P::He;
+    const FaceOutT<P> o = dir == 0 ? a.u : a.v;
+    Po* __restrict__ PoL = o.PoL + fo;
+    Po* __restrict__ PoR = o.PoR + fo;
+    Ko* __restrict__ KoL = o.KoL + fo;
+    Ko* __restrict__ KoR = o.KoR + fo;
+    He* __restrict__ hEff = o.hEff + fo;
+    const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
+
+    if (!(wet > 0.0)) {  // ocean_redi.F90:722-730: inert coefficients
+        for (int s = 0; s < ns; ++s) {
+            PoL[s * fstride] = Po(0);
+            PoR[s * fstride] = Po(0);
+            KoL[s * fstride] = Ko(1);
+            KoR[s * fstride] = Ko(1);
+        }
+        for (int s = 0; s < ns - 1; ++s) hEff[s * fstride] = He(0);
+        return;
+    }
+
+    const IfcState* XL = a.ifc + colL;
+    const IfcState* XR = a.ifc + colR;
+    const double* PL = a.pint + colL;
+    const double* PR = a.pint + colR;
+    const double pa_to_h = 1.0 / (kGravity * a.rho0);
+    const int nk = nz;
+    constexpr int kAhead = NR - 3;  // interfaces in flight beyond the window
+
+#pragma unroll
+    for (int q = 0; q < 3 + kAhead; ++q) {
+        sw_fetch(r, 0, q, XL, PL, nk, ld);
+        sw_fetch(r, 1, q, XR, PR, nk, ld);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+
+    int kL = 1, kR = 1;
+    double lastP_left = 0.0, lastP_right = 0.0;
+    int lastK_left = 1, lastK_right = 1;
+    bool reached_bottom = false, search_left = false, search_right = false;
+    double absL_prev = 0.0, absR_prev = 0.0;
+
+    for (int ks = 1; ks <= ns; ++ks) {
+        if constexpr (kAhead == 0) cp_async_wait<0>();
+        const int kl = kL, kr = kR;
+        const IfcState oL = sw_ifc(r, 0, kl - 1), oR = sw_ifc(r, 1, kr - 1);
+        const double dRho = secant_drho(oR, oL);
+        if (!reached_bottom) {
+            if (dRho < 0.0) {
+                search_left = true;
+                search_right = false;
+            } else if (dRho > 0.0) {
+                search_right = true;
+                search_left = false;
+            } else if (kl + kr == 2) {
+                search_left = true;
+                search_right = false;
+            } else {
+                search_left = !search_left;
+                search_right = !search_right;
+            }
+        }
+        const bool L = search_left;
+        const int sS = L ? 0 : 1, sA = L ? 1 : 0;
+        const int Sk = L ? kl : kr, ka = L ? kr : kl;
+        const int w0 = Sk > 2 ? Sk - 2 : 0;  // the searched column's km1, 0-based
+        const IfcState Sa = sw_ifc(r, sS, w0);
+        const IfcState anc = sw_ifc(r, sA, ka - 1);
+        const double dRhoTop = secant_drho(Sa, anc);
+        const double dRhoBot = Sk >= 2 ? (L ? -dRho : dRho) : secant_drho(sw_ifc(r, sS, w0 + 1), anc);
+        const double Spa = sw_p(r, sS, w0), Spb = sw_p(r, sS, w0 + 1);
+        const int km1 = w0 + 1;
+        double po_s;
+        const bool top_zero = (L ? (dRhoTop > 0.0) : (dRhoTop >= 0.0)) || kr + kl == 2;
+        if (top_zero) po_s = 0.0;
+        else if (dRhoTop >= dRhoBot) po_s = 1.0;
+        else po_s = interpolate_position(dRhoTop, Spa, dRhoBot, Spb);
+        int ko_s = km1;
+        bool carried = false;
+        if (po_s >= 1.0 && km1 < nk) {
+            ko_s = km1 + 1;
+            po_s = po_s - 1.0;
+            carried = true;
+        }
+        const int lastK_s = L ? lastK_left : lastK_right;
+        const double lastP_s = L ? lastP_left : lastP_right;
+        bool backstop = false;
+        if ((double)(ko_s - lastK_s) + (po_s - lastP_s) < 0.0) {
+            po_s = lastP_s;
+            ko_s = lastK_s;
+            backstop = true;
+        }
+        double abs_s;
+        if (backstop) abs_s = L ? absL_prev : absR_prev;
+        else if (carried) abs_s = Spb + po_s * (sw_p(r, sS, w0 + 2) - Spb);
+        else abs_s = Spa + po_s * (Spb - Spa);
+        double po_a, abs_a;
+        int ko_a;
+        if (ka <= nk) {
+            po_a = 0.0;
+            ko_a = ka;
+            abs_a = sw_p(r, sA, ka - 1);
+            // the anchor column advances: its window slides once k >= 2, and
+            // the slot that left it receives the interface kAhead + 2 below
+            // the one that entered
+            if (ka >= 2) {
+                if constexpr (kAhead == 2) cp_async_wait<1>();
+                else if constexpr (kAhead == 1) cp_async_wait<0>();
+                sw_fetch(r, sA, ka + kAhead + 1, L ? XR : XL, L ? PR : PL, nk, ld);
+                cp_async_commit();
+            }
+            if (L) kR = ka + 1;
+            else kL = ka + 1;
+        } else {
+            po_a = 1.0;
+            ko_a = nk;
+            const double Apa = sw_p(r, sA, ka - 2), Apb = sw_p(r, sA, ka - 1);
+            abs_a = Apa + po_a * (Apb - Apa);  // km1 = nk: interfaces nk, nk+1
+            reached_bottom = true;
+            search_left = !L;
+            search_right = L;
+        }
+        const double pol = L ? po_s : po_a, por = L ? po_a : po_s;
+        const int kol = L ? ko_s : ko_a, kor = L ? ko_a : ko_s;
+        const double absL = L ? abs_s : abs_a, absR = L ? abs_a : abs_s;
+        lastK_left = kol;
+        lastP_left = pol;
+        lastK_right = kor;
+        lastP_right = por;
+        const size_t so = (size_t)(ks - 1) * fstride;
+        PoL[so] = Po(pol);
+        PoR[so] = Po(por);
+        KoL[so] = Ko(kol);
+        KoR[so] = Ko(kor);
+        if (ks > 1) {  // harmonic-mean effective thickness (:452-462), Pa -> m (:688-691)
+            const double hL = absL - absL_prev;
+            const double hR = absR - absR_prev;
+            double he = 0.0;
+            if (hL + hR > 0.0) he = 2.0 * hL * hR / (hL + hR);
+            hEff[so - fstride] = He(he * pa_to_h);
+        }
+        absL_prev = absL;
+        absR_prev = absR;
+    }
+    cp_async_wait<0>();  // no copy may land in the ring after this face is done
 }
 
 // ---------------------------------------------------------------------------
@@ -978,6 +1212,263 @@ __device__ __forceinline__ void flux_item_staged(const FaceFluxArgsT<P>& a, int 
         staged = staged_next;
     }
     cp_async_wait<0>();  // nothing may land in the slots after this face is done
+}
+
+// ---------------------------------------------------------------------------
+// The face flux reading each column's reconstruction through a two-layer ring
+// in shared memory.
+//
+// Along a face the layer of each column's bottom surface never decreases and
+// moves by one layer at a time, so per column side the sublayer walk needs the
+// record of its current layer c (the prepared PPM layer and the interface value
+// at the layer's bottom, Ti[c]) and, when the next surface moves down, the
+// record of layer c + 1; Ti[c - 1] (the current layer's top interface) stays in
+// a register. Record c + 1 is copied into the ring (cp.async) when the side
+// enters layer c, so a sublayer that advances finds it in shared memory instead
+// of waiting on a global load whose address its own Ko gives; every layer record
+// is fetched once per face side instead of once per sublayer.
+// A sublayer whose layers the ring does not hold (the first live sublayer of a
+// face, the first after a run the whole warp skipped, a jump of more than one
+// layer) loads as flux_item does and re-primes the ring. The arithmetic, the
+// values and the stores are exactly flux_item's.
+// Per thread, structure of arrays over the block's threads:
+//   rpp [slot][side][tracer][kU][kFluxThreads] 16-byte units (PPM record),
+//   rti [slot][side][tracer][kFluxThreads] doubles (Ti at the layer's bottom),
+// slot = layer & 1.
+// ---------------------------------------------------------------------------
+template <int NT, class P>
+struct FluxRing {
+    static constexpr int kU = PpmUnits<P>::n;
+    static constexpr size_t pp_units = (size_t)2 * 2 * NT * kU * kFluxThreads;
+    static constexpr size_t ti_doubles = (size_t)2 * 2 * NT * kFluxThreads;
+    static constexpr size_t bytes = pp_units * 16 + ti_doubles * 8;
+};
+
+template <int NT, class P>
+__device__ __forceinline__ void flux_item_ring(const FaceFluxArgsT<P>& a, int dir, int t, int tr0, int t_end,
+                                               double2* __restrict__ rpp, double* __restrict__ rti) {
+    using Ops = FluxOps<P>;
+    using Raw = typename Ops::Raw;
+    using He = typename P::He;
+    using Ppm = typename P::Ppm;
+    constexpr int kU = PpmUnits<P>::n;
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    const size_t ncol = (size_t)nx * ny;
+    const int tid = threadIdx.x;
+    int colL, colR, fo;
+    size_t fstride;
+    bool valid;
+    if ((dir == 0 ? (nx - 1) * ny : nx * (ny - 1)) <= 0) return;  // no face 0 to stand in
+    if (dir == 0) {
+        valid = t < min(t_end, (nx - 1) * ny);
+        const int tt = valid ? t : 0;
+        const int j = tt / (nx - 1), fi = 1 + tt % (nx - 1);
+        const int I = fi + 1;
+        valid = valid && !((a.wall_w && I == a.nghost + 1) || (a.wall_e && I == a.nghost + a.nxp + 1));
+        colL = (fi - 1) + nx * j;
+        colR = fi + nx * j;
+        fo = fi + (nx + 1) * j;
+        fstride = (size_t)(nx + 1) * ny;
+    } else {
+        valid = t < min(t_end, nx * (ny - 1));
+        const int tt = valid ? t : 0;
+        const int fj = 1 + tt / nx, i = tt % nx;
+        const int J = fj + 1;
+        valid = valid && !((a.wall_s && J == a.nghost + 1) || (a.wall_n && J == a.nghost + a.nyp + 1));
+        colL = i + nx * (fj - 1);
+        colR = i + nx * fj;
+        fo = i + nx * fj;
+        fstride = (size_t)nx * (ny + 1);
+    }
+    if (!__any_sync(0xffffffffu, valid)) return;  // warp-uniform
+    const FaceInT<P>& c = dir == 0 ? a.u : a.v;
+    const He* __restrict__ hEff = c.hEff + fo;
+    const typename P::Po* __restrict__ PoL = c.PoL + fo;
+    const typename P::Po* __restrict__ PoR = c.PoR + fo;
+    const typename P::Ko* __restrict__ KoL = c.KoL + fo;
+    const typename P::Ko* __restrict__ KoR = c.KoR + fo;
+    const double* kh = dir == 0 ? a.khtr_u : a.khtr_v;
+    const double khv = kh ? __ldg(kh + fo) : a.khtr;
+    // ((dt*khtr)*dy)*idx, ocean_redi.F90:1156/1168
+    const double coef = a.dt * khv * __ldg((dir == 0 ? a.dy_cu : a.dx_cv) + fo) *
+                        __ldg((dir == 0 ? a.idxCu : a.idyCv) + fo);
+    const int nt = min(NT, a.ntr - tr0);
+    const size_t ti_stride = ncol * (nz + 1), pp_stride = ncol * nz, f_stride = (size_t)(ns - 1) * fstride;
+    const double* const ti0[2] = {a.ti + (size_t)tr0 * ti_stride + colL, a.ti + (size_t)tr0 * ti_stride + colR};
+    const Ppm* const pp0[2] = {a.ppm + (size_t)tr0 * pp_stride + colL, a.ppm + (size_t)tr0 * pp_stride + colR};
+    typename P::Flux* const Fo0 = (dir == 0 ? a.Fu : a.Fv) + fo;
+    auto trc = [nt](int n) { return (size_t)(n < nt ? n : 0); };
+    auto pp_at = [&](int layer, int side, int n) {
+        return rpp + ((size_t)((((layer & 1) * 2 + side) * NT + n) * kU)) * kFluxThreads + tid;
+    };
+    auto ti_at = [&](int layer, int side, int n) {
+        return rti + ((size_t)(((layer & 1) * 2 + side) * NT + n)) * kFluxThreads + tid;
+    };
+    // record of layer k (1-based; clamped to the column) of one side
+    auto fetch = [&](int side, int k) {
+        const int kc = min(k, nz);
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+            const char* src = reinterpret_cast<const char*>(pp0[side] + trc(n) * pp_stride + (size_t)(kc - 1) * ncol);
+#pragma unroll
+            for (int u = 0; u < kU; ++u) cp_async16_ca(pp_at(k, side, n) + (size_t)u * kFluxThreads, src + 16 * u);
+            cp_async8(ti_at(k, side, n), ti0[side] + trc(n) * ti_stride + (size_t)kc * ncol);
+        }
+    };
+    auto gti = [&](int side, int n, int k) { return __ldg(ti0[side] + trc(n) * ti_stride + (size_t)k * ncol); };
+
+    bool have_t = false;  // warp-uniform
+    int kl_t = min(max((int)__ldg(KoL), 1), nz), kr_t = min(max((int)__ldg(KoR), 1), nz);
+    double pl_t = __ldg(PoL), pr_t = __ldg(PoR);
+    He he_c = __ldg(hEff);
+    int klr_c = __ldg(KoL + fstride), krr_c = __ldg(KoR + fstride);
+    double pl_c = __ldg(PoL + fstride), pr_c = __ldg(PoR + fstride);
+    int cur[2] = {0, 0};    // layer whose record the ring holds as current (0: none)
+    // what the newest copy group (the last live sublayer's) holds per side:
+    // 1 the record below the current layer (an advance), 2 both (a re-prime)
+    int newest[2] = {0, 0};
+    double ttop[2][NT];     // Ti at the current layer's top interface
+    double tl[NT], tr[NT];  // the top surface's tracer values
+#pragma unroll
+    for (int n = 0; n < NT; ++n) ttop[0][n] = ttop[1][n] = 0.0;
+    for (int s = 0; s < ns - 1; ++s) {
+        const size_t s0 = (size_t)s * fstride;
+        He he_n = He(0);
+        int klr_n = 1, krr_n = 1;
+        double pl_n = 0.0, pr_n = 0.0;
+        if (s + 1 < ns - 1) {
+            const size_t s2 = s0 + 2 * fstride;
+            he_n = __ldg(hEff + s0 + fstride);
+            klr_n = __ldg(KoL + s2);
+            krr_n = __ldg(KoR + s2);
+            pl_n = __ldg(PoL + s2);
+            pr_n = __ldg(PoR + s2);
+        }
+        const int kb[2] = {min(max(klr_c, 1), nz), min(max(krr_c, 1), nz)};
+        const int kt[2] = {kl_t, kr_t};
+        const double pt[2] = {pl_t, pr_t}, pb[2] = {pl_c, pr_c};
+        const bool live = valid && he_c != He(0);
+        if (!__any_sync(0xffffffffu, live)) {
+#pragma unroll
+            for (int n = 0; n < NT; ++n)
+                if (valid && n < nt) Fo0[(size_t)n * f_stride + s0] = typename P::Flux(0);
+            have_t = false;
+        } else {
+            bool fast[2], adv[2];
+#pragma unroll
+            for (int d = 0; d < 2; ++d) {
+                fast[d] = cur[d] == kt[d] && (kb[d] == kt[d] || kb[d] == kt[d] + 1);
+                adv[d] = fast[d] && kb[d] != kt[d];
+            }
+            const double xR[2] = {pb[0] + (double)(kb[0] - kt[0]), pb[1] + (double)(kb[1] - kt[1])};
+            if (__all_sync(0xffffffffu, fast[0] && fast[1])) {
+                // Every lane reads its ring. Every group but the newest is
+                // complete after wait_group 1; the newest is waited for when
+                // this sublayer reads from it: the current record after a
+                // re-prime, the one below after an advance.
+                bool need0 = false;
+#pragma unroll
+                for (int d = 0; d < 2; ++d) need0 = need0 || newest[d] == 2 || (adv[d] && newest[d] == 1);
+                if (need0) cp_async_wait<0>();
+                else cp_async_wait<1>();
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    double b0[2], b1[2];
+                    Raw q[2];
+#pragma unroll
+                    for (int d = 0; d < 2; ++d) {
+                        const double tk = *ti_at(kt[d], d, n);                       // Ti[kt]
+                        b1[d] = *ti_at(adv[d] ? kt[d] + 1 : kt[d], d, n);            // Ti[kb]
+                        b0[d] = adv[d] ? tk : ttop[d][n];                            // Ti[kb - 1]
+                        q[d] = ld_stage_ppm<P>(pp_at(kt[d], d, n));
+                        if (!have_t) {
+                            const double top = interp(pt[d], ttop[d][n], tk);
+                            if (d == 0) tl[n] = top;
+                            else tr[n] = top;
+                        }
+                        ttop[d][n] = b0[d];
+                    }
+                    const double bl = interp(pb[0], b0[0], b1[0]);
+                    const double br = interp(pb[1], b0[1], b1[1]);
+                    if (valid && n < nt) {
+                        const typename Ops::Mean tlay = Ops::mean(pt[0], xR[0], q[0]);
+                        const typename Ops::Mean trlay = Ops::mean(pt[1], xR[1], q[1]);
+                        const double dT = guarded_dT(tr[n] - tl[n], br - bl, (double)(trlay - tlay));
+                        Fo0[(size_t)n * f_stride + s0] = he_c == He(0) ? typename P::Flux(0) : Ops::flux(dT, he_c, coef);
+                    }
+                    tl[n] = bl;
+                    tr[n] = br;
+                    // shared-memory reads wait tens of cycles: one tracer's at a
+                    // time keeps the registers of the others free
+                    if (n + 1 < NT) asm volatile("" ::: "memory");
+                }
+                // an advancing side fetches the layer below its new one into the
+                // slot it leaves (read above, so its copy is complete)
+#pragma unroll
+                for (int d = 0; d < 2; ++d) {
+                    newest[d] = adv[d] ? 1 : 0;
+                    if (adv[d]) {
+                        fetch(d, kb[d] + 1);
+                        cur[d] = kb[d];
+                    }
+                }
+            } else {
+                // Some lane is off its ring: every lane loads as flux_item does,
+                // then re-primes both sides at their bottom layers once none of
+                // its copies is in flight (no slot may have two).
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    double b0[2], b1[2];
+                    Raw q[2];
+#pragma unroll
+                    for (int d = 0; d < 2; ++d) {
+                        b0[d] = gti(d, n, kb[d] - 1);
+                        b1[d] = gti(d, n, kb[d]);
+                        q[d] = Ops::template load<LdNC>(pp0[d] + trc(n) * pp_stride + (size_t)(kt[d] - 1) * ncol);
+                    }
+                    if (!have_t) {
+                        tl[n] = interp(pt[0], gti(0, n, kt[0] - 1), gti(0, n, kt[0]));
+                        tr[n] = interp(pt[1], gti(1, n, kt[1] - 1), gti(1, n, kt[1]));
+                    }
+                    const double bl = interp(pb[0], b0[0], b1[0]);
+                    const double br = interp(pb[1], b0[1], b1[1]);
+                    if (valid && n < nt) {
+                        const typename Ops::Mean tlay = Ops::mean(pt[0], xR[0], q[0]);
+                        const typename Ops::Mean trlay = Ops::mean(pt[1], xR[1], q[1]);
+                        const double dT = guarded_dT(tr[n] - tl[n], br - bl, (double)(trlay - tlay));
+                        Fo0[(size_t)n * f_stride + s0] = he_c == He(0) ? typename P::Flux(0) : Ops::flux(dT, he_c, coef);
+                    }
+                    tl[n] = bl;
+                    tr[n] = br;
+#pragma unroll
+                    for (int d = 0; d < 2; ++d) ttop[d][n] = b0[d];
+                    // one tracer's loads at a time: this path is rare, and its
+                    // register peak would otherwise set the kernel's
+                    if (n + 1 < NT) asm volatile("" ::: "memory");
+                }
+                cp_async_wait<0>();
+#pragma unroll
+                for (int d = 0; d < 2; ++d) {
+                    fetch(d, kb[d]);
+                    fetch(d, kb[d] + 1);
+                    cur[d] = kb[d];
+                    newest[d] = 2;
+                }
+            }
+            cp_async_commit();
+            have_t = true;
+        }
+        kl_t = kb[0];
+        kr_t = kb[1];
+        pl_t = pl_c;
+        pr_t = pr_c;
+        he_c = he_n;
+        klr_c = klr_n;
+        krr_c = krr_n;
+        pl_c = pl_n;
+        pr_c = pr_n;
+    }
+    cp_async_wait<0>();  // nothing may land in the ring after this face is done
 }
 
 // ---------------------------------------------------------------------------

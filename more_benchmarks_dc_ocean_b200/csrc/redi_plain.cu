@@ -18,7 +18,9 @@
 //                      of its up to four faces).
 //     k_neutral_sweep  one thread per interior wet face: the 2nz+2-surface
 //                      continuous sweep (ocean_redi.F90:307-464), writing
-//                      PoL/PoR/KoL/KoR/hEff in the reference layout.
+//                      PoL/PoR/KoL/KoR/hEff in the reference layout
+//                      (k_neutral_sweep_w: both columns' windows in a
+//                      shared-memory ring, the default).
 //
 //   Phase B  redi_apply_flux (ocean_redi.F90:927-1181), all tracers fused
 //     k_tracer_recon   one thread per (column, tracer pair): top-down PPM tracer
@@ -62,6 +64,16 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgsT<P> a, FaceRang
     if (t < r.hi[d]) sweep_item<P, LdNC, true>(a, d, t);
 }
 
+// The sweep with both windows in a shared-memory ring of NR interfaces per
+// column (dynamic shared memory: sizeof(SweepWin<NR>)).
+template <class P, int NR>
+__global__ void __launch_bounds__(128) k_neutral_sweep_w(SweepArgsT<P> a, FaceRange r) {
+    extern __shared__ __align__(16) unsigned char sweep_win[];
+    const int d = blockIdx.x & 1;
+    const int t = r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
+    if (t < r.hi[d]) sweep_item_win<P, LdNC, NR>(a, d, t, *reinterpret_cast<SweepWin<NR>*>(sweep_win));
+}
+
 template <int NT, class P>
 __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgsT<P> a, int c0, int nb) {
     recon_item<NT, P, LdNC>(a, blockIdx.x * blockDim.x + threadIdx.x, c0, nb);
@@ -79,6 +91,17 @@ __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0, 
 
 // The face flux with its reconstruction loads staged one sublayer ahead
 // through shared memory (flux_item_staged); the same block order.
+// The face flux reading each column's reconstruction through a two-layer ring
+// in shared memory (flux_item_ring); the same block order.
+template <int NT, class P>
+__global__ void __launch_bounds__(kFluxThreads) k_face_flux_r(FaceFluxArgsT<P> a, int tr0, FaceRange r) {
+    extern __shared__ __align__(16) unsigned char ring[];
+    double2* rpp = reinterpret_cast<double2*>(ring);
+    double* rti = reinterpret_cast<double*>(ring + FluxRing<NT, P>::pp_units * sizeof(double2));
+    const int d = blockIdx.x & 1;
+    flux_item_ring<NT, P>(a, d, r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x, tr0, r.hi[d], rpp, rti);
+}
+
 template <int NT, class P>
 __global__ void __launch_bounds__(kFluxThreads) k_face_flux_s(FaceFluxArgsT<P> a, int tr0, FaceRange r) {
     extern __shared__ __align__(16) unsigned char stage[];
@@ -182,14 +205,32 @@ cudaError_t launch_eos_points(const EosParams& e, int n, const double* T, const 
     return cudaGetLastError();
 }
 
+template <class P, int NR>
+static cudaError_t launch_sweep_w(const SweepArgsT<P>& sw, const plain::FaceRange& f, unsigned nb, cudaStream_t st) {
+    const size_t smem = sizeof(plain::SweepWin<NR>);
+    cudaError_t e =
+        cudaFuncSetAttribute(plain::k_neutral_sweep_w<P, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    plain::k_neutral_sweep_w<P, NR><<<2 * nb, plain::kSweepThreads, smem, st>>>(sw, f);
+    return cudaSuccess;
+}
+
 template <class P>
 cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st, Band band) {
     const BandRanges r = band_ranges(sw.nx, sw.ny, band);
     const unsigned nb = face_blocks(r.f);
     if (nb > 0) {
         const int kid = P::kMixed ? K_MIXED_SWEEP : K_NEUTRAL_SWEEP;
+        const int form = cell_tuning().sweep_form;
         launch_begin(kid, st);
-        plain::k_neutral_sweep<P><<<2 * nb, 128, 0, st>>>(sw, r.f);
+        if (form >= 3 && form <= 5) {
+            cudaError_t e = form == 3   ? launch_sweep_w<P, 3>(sw, r.f, nb, st)
+                            : form == 4 ? launch_sweep_w<P, 4>(sw, r.f, nb, st)
+                                        : launch_sweep_w<P, 5>(sw, r.f, nb, st);
+            if (e != cudaSuccess) return e;
+        } else {
+            plain::k_neutral_sweep<P><<<2 * nb, 128, 0, st>>>(sw, r.f);
+        }
         launch_end(kid, st);
     }
     return cudaGetLastError();
@@ -236,8 +277,27 @@ static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT
     const unsigned nb = face_blocks(r.f);
     if (nb > 0) {
         const int kid = P::kMixed ? K_MIXED_FLUX : K_FACE_FLUX;
-        if constexpr (NT <= 2) {
-            if (tune.flux_staged) {
+        bool done = false;
+        if constexpr (NT <= 4) {
+            if (tune.flux_staged == 2) {
+                static int opted[64] = {};
+                int dev = 0;
+                cudaGetDevice(&dev);
+                const int bytes = (int)plain::FluxRing<NT, P>::bytes;
+                if (dev >= 0 && dev < 64 && !opted[dev]) {
+                    cudaFuncSetAttribute(plain::k_face_flux_r<NT, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes);
+                    opted[dev] = 1;
+                }
+                launch_begin(kid, st);
+                plain::k_face_flux_r<NT, P><<<2 * nb, plain::kFluxThreads, bytes, st>>>(ff, tr0, r.f);
+                launch_end(kid, st);
+                done = true;
+            }
+        }
+        if (done) {
+        } else if constexpr (NT <= 2) {
+            if (tune.flux_staged == 1) {
                 // opt into more than 48 KB of dynamic shared memory once per device
                 static int opted[64] = {};
                 int dev = 0;
@@ -415,8 +475,10 @@ cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, 
         launch_recon<P>(rc, r, st);
     }
     const CellTuning tune = cell_tuning();
-    // the staged face flux holds one or two tracers' reconstruction in shared memory
-    const int group = tracer_group(ff.ntr, tune.flux_staged ? (tune.group < 2 ? tune.group : 2) : tune.group);
+    // the staged face flux holds one or two tracers' reconstruction in shared
+    // memory, the ring form up to four
+    const int cap = tune.flux_staged == 1 ? 2 : (tune.flux_staged == 2 ? 4 : 8);
+    const int group = tracer_group(ff.ntr, tune.group < cap ? tune.group : cap);
     for (int tr0 = 0; tr0 < ff.ntr; tr0 += group) {
         switch (group) {
             case 8: launch_flux_gather<8, P>(ff, cg, tr0, r, tune, st); break;

@@ -304,10 +304,12 @@ def test_gather_forms_match_oracle(redi_lib, oracle_lib, gnt, smem, chunk):
         autotune.set_tracer_group(saved[2])
 
 
-@pytest.mark.parametrize("group,precision", [(1, 0), (2, 0), (2, 1)])
-def test_staged_face_flux_matches(redi_lib, oracle_lib, group, precision):
-    """The face flux with its reconstruction staged through shared memory one sublayer ahead:
-    FP64 equals the oracle bit for bit; the mixed form equals the unstaged mixed form bit for bit."""
+@pytest.mark.parametrize("form,group,precision", [(1, 1, 0), (1, 2, 0), (1, 2, 1), (2, 1, 0), (2, 2, 0), (2, 4, 0),
+                                                   (2, 2, 1), (2, 4, 1)])
+def test_staged_face_flux_matches(redi_lib, oracle_lib, form, group, precision):
+    """The face flux with its reconstruction staged through shared memory one sublayer ahead
+    (form 1) or read through a two-layer ring per column side (form 2): FP64 equals the oracle
+    bit for bit; the mixed form equals the plain mixed form bit for bit."""
     from more_benchmarks_dc_ocean_b200 import autotune
 
     R = redi_lib
@@ -323,7 +325,7 @@ def test_staged_face_flux_matches(redi_lib, oracle_lib, group, precision):
             torch.cuda.synchronize()
             ref = [t.cpu().numpy() for t in dp.ms.tracers]
             redi.destroy()
-            autotune.set_flux_staged(True)
+            autotune.set_flux_staged(form)
             dp = R.to_device(p)
             redi = R.make_redi(dp, R.MIXED)
             R.step(dp, redi, 1)
@@ -332,11 +334,100 @@ def test_staged_face_flux_matches(redi_lib, oracle_lib, group, precision):
             assert redi.error_count() == 0
             redi.destroy()
         else:
-            autotune.set_flux_staged(True)
+            autotune.set_flux_staged(form)
             _, got = _run_gpu(p, 1, redi_lib, check_coeffs=False)
             _, ref = _run_oracle(p, 1)
         for n, (a, b) in enumerate(zip(got, ref)):
-            _assert_exact(f"staged flux group={group} precision={precision} tracer {n}", a, b)
+            _assert_exact(f"flux form={form} group={group} precision={precision} tracer {n}", a, b)
     finally:
         autotune.set_flux_staged(saved[0])
         autotune.set_tracer_group(saved[1])
+
+
+_SWEEP_CASES = {
+    "config0": lambda: inputs.config0(),
+    "tie_break": lambda: _uniform_problem(),
+    "vanished": lambda: _vanished_problem(),
+    "nz1": lambda: inputs.make_problem(17, 13, 1, n_seamounts=3, land_fraction=0.2, seed=12),
+    "nz2": lambda: inputs.make_problem(17, 13, 2, n_seamounts=3, land_fraction=0.2, seed=13),
+}
+
+
+def _uniform_problem():
+    p = inputs.make_problem(12, 10, 6, n_seamounts=0, land_fraction=0.0, seed=3)
+    p.h[:] = 100.0
+    zc = (np.arange(6)[::-1] + 0.5) * 100.0
+    for n, base in enumerate((10.0, 35.0)):
+        p.tracers[n][:] = (base + 0.001 * zc)[:, None, None] * 100.0
+    return p
+
+
+def _vanished_problem():
+    p = inputs.make_problem(20, 16, 8, n_seamounts=4, land_fraction=0.5, seed=21)
+    mask = np.random.default_rng(0).random(p.h.shape) < 0.15
+    p.h[mask] = 0.0
+    for t in p.tracers:
+        t[mask] = 0.0
+    return p
+
+
+@pytest.mark.parametrize("form", [0, 3, 4, 5])
+@pytest.mark.parametrize("case", sorted(_SWEEP_CASES))
+def test_sweep_forms_match_oracle(redi_lib, oracle_lib, form, case):
+    """Every neutral-sweep form (register windows; windows in a shared-memory ring of 3, 4 or 5
+    interfaces) gives the oracle's coefficients and tracers bit for bit over two steps."""
+    from more_benchmarks_dc_ocean_b200 import autotune
+
+    saved = autotune.get_sweep_form()
+    try:
+        autotune.set_sweep_form(form)
+        _compare(_SWEEP_CASES[case](), 2, redi_lib)
+    finally:
+        autotune.set_sweep_form(saved)
+
+
+@pytest.mark.parametrize("form", [3, 4, 5])
+def test_sweep_forms_mixed_match_register_form(redi_lib, form):
+    """The mixed-precision step (FP64 sweep decisions, narrower coefficient storage) does not
+    depend on the sweep form either: tracers after two steps equal bit for bit."""
+    from more_benchmarks_dc_ocean_b200 import autotune
+
+    R = redi_lib
+    saved = autotune.get_sweep_form()
+    p = inputs.make_problem(41, 33, 23, n_seamounts=5, land_fraction=0.3, seed=77)
+    out = []
+    try:
+        for f in (0, form):
+            autotune.set_sweep_form(f)
+            dp = R.to_device(p)
+            redi = R.make_redi(dp, R.MIXED)
+            R.step(dp, redi, 2)
+            torch.cuda.synchronize()
+            assert redi.error_count() == 0
+            out.append([t.cpu().numpy() for t in dp.ms.tracers])
+            redi.destroy()
+    finally:
+        autotune.set_sweep_form(saved)
+    for n, (a, b) in enumerate(zip(out[1], out[0])):
+        _assert_exact(f"mixed sweep form {form} tracer {n}", a, b)
+
+
+def test_sweep_form_rejects_unknown(redi_lib):
+    from more_benchmarks_dc_ocean_b200 import autotune
+
+    with pytest.raises(Exception):
+        autotune.set_sweep_form(2)
+
+
+@pytest.mark.parametrize("case", ["tie_break", "vanished", "nz1", "nz2"])
+def test_ring_face_flux_edge_cases(redi_lib, oracle_lib, case):
+    """The ring face flux on the sweep's edge cases (uniform fields, vanished layers and land,
+    one- and two-layer columns), two steps, bit for bit."""
+    from more_benchmarks_dc_ocean_b200 import autotune
+
+    saved = autotune.get_flux_staged()
+    try:
+        autotune.set_flux_staged(2)
+        _compare(_SWEEP_CASES[case](), 2, redi_lib)
+    finally:
+        autotune.set_flux_staged(saved)
