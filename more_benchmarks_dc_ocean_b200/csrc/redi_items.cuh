@@ -43,18 +43,24 @@ __device__ __forceinline__ void finish_layer(const RawLayer<NS>& r, double& hv, 
     for (int n = 0; n < NS; ++n) sv[n] = r.s[n] / he;
 }
 
-template <int NS, class Fetch, class Emit>
+// AHEAD = 2 keeps a second raw layer in flight (layer t+3 requested while t is
+// formed), so every load has two iterations to arrive.
+template <int NS, class Fetch, class Emit, int AHEAD = 1>
 __device__ __forceinline__ void stream_edges(int nk, Fetch fetch, Emit emit) {
+    static_assert(AHEAD == 1 || AHEAD == 2, "one or two raw layers in flight");
     double hA = 0.0, hB, hC, hD = 0.0;  // h(t-2), h(t-1), h(t), h(t+1)
     double sB[NS], sC[NS], sD[NS];      // layer scalars t-1, t, t+1
     double dB[NS], dC[NS];              // PLM slopes of layers t-1, t
     double e[NS];
-    RawLayer<NS> r1, r2, rn;            // rn: raw layer t+2, in flight
+    RawLayer<NS> r1, r2, rn, rn2;       // rn: raw layer t+2 in flight; rn2: t+3 (AHEAD 2)
 
     // t = 1: edge(1) = tr(1) - 0.5*diff(1), diff(1) = 0.
     fetch(1, r1);
     if (nk >= 2) fetch(2, r2);
     if (nk >= 3) fetch(3, rn);
+    if constexpr (AHEAD == 2) {
+        if (nk >= 4) fetch(4, rn2);
+    }
     finish_layer(r1, hC, sC);
     if (nk >= 2) finish_layer(r2, hD, sD);
 #pragma unroll
@@ -78,7 +84,12 @@ __device__ __forceinline__ void stream_edges(int nk, Fetch fetch, Emit emit) {
         }
         if (t + 1 <= nk) {
             finish_layer(rn, hD, sD);
-            if (t + 2 <= nk) fetch(t + 2, rn);
+            if constexpr (AHEAD == 2) {
+                if (t + 2 <= nk) rn = rn2;
+                if (t + 3 <= nk) fetch(t + 3, rn2);
+            } else {
+                if (t + 2 <= nk) fetch(t + 2, rn);
+            }
         }
         // diff(t): PLM slope for 2 <= t <= nk-1, PCM (0) at t = nk.
         if (t <= nk - 1) {
@@ -106,6 +117,11 @@ __device__ __forceinline__ void stream_edges(int nk, Fetch fetch, Emit emit) {
 // Phase A, step 1: per-column interface state (redi_build_column,
 // ocean_redi.F90:609-654), written in [interface][column] order.
 // ---------------------------------------------------------------------------
+// Raw layers in flight per column thread (stream_edges' AHEAD) in the column
+// state and reconstruction passes.
+constexpr int kColumnAhead = 1;
+constexpr int kReconAhead = 1;
+
 template <class LD>
 __device__ __forceinline__ void column_state_item(const ColumnStateArgs& a, int col) {
     const int ncol = a.nx * a.ny;
@@ -143,7 +159,7 @@ __device__ __forceinline__ void column_state_item(const ColumnStateArgs& a, int 
         pint[(size_t)(t - 1) * ncol] = P;
         h_layer_above = h_t;
     };
-    stream_edges<2>(nz, fetch, emit);
+    stream_edges<2, decltype(fetch), decltype(emit), kColumnAhead>(nz, fetch, emit);
 }
 
 // ---------------------------------------------------------------------------
@@ -489,11 +505,12 @@ __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int 
 // reaches a decision (every use compares with 0 or forms a difference with a
 // non-zero value).
 // ---------------------------------------------------------------------------
+constexpr int kSweepWinThreads = 128;  // block size of the shared-memory-window sweep
 template <int NR>
 struct SweepWin {
-    double2 ts[NR][2][kSweepThreads];  // (T, S)
-    double2 dd[NR][2][kSweepThreads];  // (dR/dT, dR/dS)
-    double p[NR][2][kSweepThreads];    // pressure
+    double2 ts[NR][2][kSweepWinThreads];  // (T, S)
+    double2 dd[NR][2][kSweepWinThreads];  // (dR/dT, dR/dS)
+    double p[NR][2][kSweepWinThreads];    // pressure
 };
 
 template <int NR>
@@ -759,7 +776,7 @@ __device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid, int 
             e_prev[n] = e[n];
         }
     };
-    stream_edges<NT>(nz, fetch, emit);
+    stream_edges<NT, decltype(fetch), decltype(emit), kReconAhead>(nz, fetch, emit);
 }
 
 // ---------------------------------------------------------------------------

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgsT<P> a, FaceRang
 // The sweep with both windows in a shared-memory ring of NR interfaces per
 // column (dynamic shared memory: sizeof(SweepWin<NR>)).
 template <class P, int NR>
-__global__ void __launch_bounds__(128) k_neutral_sweep_w(SweepArgsT<P> a, FaceRange r) {
+__global__ void __launch_bounds__(kSweepWinThreads) k_neutral_sweep_w(SweepArgsT<P> a, FaceRange r) {
     extern __shared__ __align__(16) unsigned char sweep_win[];
     const int d = blockIdx.x & 1;
     const int t = r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
@@ -211,7 +211,8 @@ static cudaError_t launch_sweep_w(const SweepArgsT<P>& sw, const plain::FaceRang
     cudaError_t e =
         cudaFuncSetAttribute(plain::k_neutral_sweep_w<P, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    plain::k_neutral_sweep_w<P, NR><<<2 * nb, plain::kSweepThreads, smem, st>>>(sw, f);
+    const unsigned nbw = (unsigned)(((size_t)nb * 128 + plain::kSweepWinThreads - 1) / plain::kSweepWinThreads);
+    plain::k_neutral_sweep_w<P, NR><<<2 * nbw, plain::kSweepWinThreads, smem, st>>>(sw, f);
     return cudaSuccess;
 }
 
