@@ -345,13 +345,15 @@ def run_b200(args, rank, world, local_rank):
     if tiling is not None:
         p = tiling.local_problem(p)
     prec = R.FP64 if args.precision == "fp64" else R.MIXED
-    if args.fold or args.flux_staged:
+    if args.fold or args.flux_staged or args.sweep_form is not None:
         from more_benchmarks_dc_ocean_b200 import autotune
 
         if args.fold:
             autotune.set_fold(autotune.FOLD_FP64 | autotune.FOLD_MIXED)
         if args.flux_staged:
-            autotune.set_flux_staged(True)
+            autotune.set_flux_staged(args.flux_staged)
+        if args.sweep_form is not None:
+            autotune.set_sweep_form(args.sweep_form)
     dp = R.to_device(p, dev)
     redi = R.make_redi(dp, prec)
     ex = None
@@ -1392,8 +1394,11 @@ def main():
     ap.add_argument("--no-sub", action="store_true", help="skip the mixed (config 2) and batched (config 3) sub-records")
     ap.add_argument("--fold", action="store_true",
                     help="Phase B as the fused face-flux + fold pass instead of the face-flux / cell-gather pair")
-    ap.add_argument("--flux-staged", action="store_true",
-                    help="the face flux with its reconstruction staged through shared memory")
+    ap.add_argument("--flux-staged", type=int, nargs="?", const=1, default=0, choices=(0, 1, 2),
+                    help="face flux form: 1 the next sublayer's reconstruction staged through shared memory, "
+                         "2 each column's reconstruction read through a two-layer shared-memory ring")
+    ap.add_argument("--sweep-form", type=int, default=None, choices=(0, 3, 4, 5),
+                    help="neutral sweep form: 0 register windows, 3/4/5 windows in a shared-memory ring")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--domains", type=int, default=64, help="config4: number of regional domains")
