@@ -200,11 +200,6 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
 }
-// L1-allocating 16-byte copy (a warp's left and right columns overlap)
-__device__ __forceinline__ void cp_async16_ca(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
@@ -1328,7 +1323,7 @@ __device__ __forceinline__ void flux_item_ring(const FaceFluxArgsT<P>& a, int di
         for (int n = 0; n < NT; ++n) {
             const char* src = reinterpret_cast<const char*>(pp0[side] + trc(n) * pp_stride + (size_t)(kc - 1) * ncol);
 #pragma unroll
-            for (int u = 0; u < kU; ++u) cp_async16_ca(pp_at(k, side, n) + (size_t)u * kFluxThreads, src + 16 * u);
+            for (int u = 0; u < kU; ++u) cp_async16(pp_at(k, side, n) + (size_t)u * kFluxThreads, src + 16 * u);
             cp_async8(ti_at(k, side, n), ti0[side] + trc(n) * ti_stride + (size_t)kc * ncol);
         }
     };
