@@ -328,25 +328,28 @@ struct redi_b200 {
     void *uKoL = nullptr, *uKoR = nullptr, *vKoL = nullptr, *vKoR = nullptr;
     void *uhEff = nullptr, *vhEff = nullptr;
     double *khtr_u = nullptr, *khtr_v = nullptr;
+    // dry-face record written by the sweep next to the coefficients (0 until
+    // the first redi_calc_coeffs: every face processed)
+    uint8_t *udry = nullptr, *vdry = nullptr;
     template <class P>
     redi::FaceOutT<P> out_u() {
         return {uPoL, uPoR, static_cast<typename P::Ko*>(uKoL), static_cast<typename P::Ko*>(uKoR),
-                static_cast<typename P::He*>(uhEff)};
+                static_cast<typename P::He*>(uhEff), udry};
     }
     template <class P>
     redi::FaceOutT<P> out_v() {
         return {vPoL, vPoR, static_cast<typename P::Ko*>(vKoL), static_cast<typename P::Ko*>(vKoR),
-                static_cast<typename P::He*>(vhEff)};
+                static_cast<typename P::He*>(vhEff), vdry};
     }
     template <class P>
     redi::FaceInT<P> in_u() {
         auto o = out_u<P>();
-        return {o.PoL, o.PoR, o.KoL, o.KoR, o.hEff};
+        return {o.PoL, o.PoR, o.KoL, o.KoR, o.hEff, o.dry};
     }
     template <class P>
     redi::FaceInT<P> in_v() {
         auto o = out_v<P>();
-        return {o.PoL, o.PoR, o.KoL, o.KoR, o.hEff};
+        return {o.PoL, o.PoR, o.KoL, o.KoR, o.hEff, o.dry};
     }
     Scratch ws;
     HostPipeline host;
@@ -546,6 +549,7 @@ int redi_b200_init(const redi_b200_grid* grid, int nz_ml, int precision, redi_b2
     A((void**)&s->vPoL, nv * ns * 8); A((void**)&s->vPoR, nv * ns * 8); A(&s->vhEff, nv * (ns - 1) * hb);
     A(&s->vKoL, nv * ns * kb); A(&s->vKoR, nv * ns * kb);
     A((void**)&s->khtr_u, nu * 8); A((void**)&s->khtr_v, nv * 8);
+    A((void**)&s->udry, nu); A((void**)&s->vdry, nv);
     if (e != cudaSuccess) {
         s->free_all();
         delete s;
@@ -566,6 +570,8 @@ int redi_b200_init(const redi_b200_grid* grid, int nz_ml, int precision, redi_b2
     }
     cudaMemsetAsync(s->khtr_u, 0, nu * 8, st);
     cudaMemsetAsync(s->khtr_v, 0, nv * 8, st);
+    cudaMemsetAsync(s->udry, 0, nu, st);
+    cudaMemsetAsync(s->vdry, 0, nv, st);
     cudaError_t e2 = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = e2;
     if (e == cudaSuccess) e = cudaGetLastError();

@@ -334,6 +334,7 @@ __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int 
     Ko* __restrict__ KoR = o.KoR + fo;
     He* __restrict__ hEff = o.hEff + fo;
     const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
+    if (o.dry) o.dry[fo] = wet > 0.0 ? 0 : 1;
 
     if (!(wet > 0.0)) {  // ocean_redi.F90:722-730: inert coefficients
         for (int s = 0; s < ns; ++s) {
@@ -568,6 +569,7 @@ __device__ __forceinline__ void sweep_item_win(const SweepArgsT<P>& a, int dir, 
     Ko* __restrict__ KoR = o.KoR + fo;
     He* __restrict__ hEff = o.hEff + fo;
     const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
+    if (o.dry) o.dry[fo] = wet > 0.0 ? 0 : 1;
 
     if (!(wet > 0.0)) {  // ocean_redi.F90:722-730: inert coefficients
         for (int s = 0; s < ns; ++s) {
@@ -873,6 +875,11 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
         fo = i + nx * fj;
         fstride = (size_t)nx * (ny + 1);
     }
+    {   // a dry face (inert coefficients) has only +0.0 fluxes: nothing is
+        // stored and the gather skips it
+        const uint8_t* dry = dir == 0 ? a.u.dry : a.v.dry;
+        if (dry && valid && dry[fo]) valid = false;
+    }
     if (!__any_sync(0xffffffffu, valid)) return;  // warp-uniform
     const FaceInT<P>& c = dir == 0 ? a.u : a.v;
     const He* __restrict__ hEff = c.hEff + fo;
@@ -1078,6 +1085,11 @@ __device__ __forceinline__ void flux_item_staged(const FaceFluxArgsT<P>& a, int 
         colR = i + nx * fj;
         fo = i + nx * fj;
         fstride = (size_t)nx * (ny + 1);
+    }
+    {   // a dry face (inert coefficients) has only +0.0 fluxes: nothing is
+        // stored and the gather skips it
+        const uint8_t* dry = dir == 0 ? a.u.dry : a.v.dry;
+        if (dry && valid && dry[fo]) valid = false;
     }
     if (!__any_sync(0xffffffffu, valid)) return;  // warp-uniform
     const FaceInT<P>& c = dir == 0 ? a.u : a.v;
@@ -1291,6 +1303,11 @@ __device__ __forceinline__ void flux_item_ring(const FaceFluxArgsT<P>& a, int di
         colR = i + nx * fj;
         fo = i + nx * fj;
         fstride = (size_t)nx * (ny + 1);
+    }
+    {   // a dry face (inert coefficients) has only +0.0 fluxes: nothing is
+        // stored and the gather skips it
+        const uint8_t* dry = dir == 0 ? a.u.dry : a.v.dry;
+        if (dry && valid && dry[fo]) valid = false;
     }
     if (!__any_sync(0xffffffffu, valid)) return;  // warp-uniform
     const FaceInT<P>& c = dir == 0 ? a.u : a.v;
@@ -1575,11 +1592,22 @@ __device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, 
     const size_t ustride = (size_t)(nx + 1) * ny, vstride = (size_t)nx * (ny + 1);
     // Faces in the reference order: W (u-face I, this cell RIGHT), E (u-face
     // I+1, LEFT), S (v-face J, RIGHT), N (v-face J+1, LEFT).
-    const bool on[4] = {I >= 2 && !((a.wall_w && I == wuf_w) || (a.wall_e && I == wuf_e)),
-                        I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e)),
-                        J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n)),
-                        J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))};
+    bool on[4] = {I >= 2 && !((a.wall_w && I == wuf_w) || (a.wall_e && I == wuf_e)),
+                  I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e)),
+                  J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n)),
+                  J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))};
     const int fo[4] = {i + (nx + 1) * j, i + 1 + (nx + 1) * j, i + nx * j, i + nx * (j + 1)};
+    // dry faces (inert coefficients, recorded by the sweep) carry only +0.0
+    // fluxes, which the face flux does not store: adding them would leave
+    // every sum unchanged, so the walk skips them
+    if (a.u.dry) {
+        on[0] = on[0] && !a.u.dry[fo[0]];
+        on[1] = on[1] && !a.u.dry[fo[1]];
+    }
+    if (a.v.dry) {
+        on[2] = on[2] && !a.v.dry[fo[2]];
+        on[3] = on[3] && !a.v.dry[fo[3]];
+    }
     const double iaij = 1.0 / LD::ld(a.areaT + col);
     int ptr[4] = {0, 0, 0, 0};
     int bad = 0;
@@ -1690,11 +1718,22 @@ __device__ __forceinline__ void gather_item_s(const CellGatherArgsT<P>& a, int i
     const int wuf_w = a.nghost + 1, wuf_e = a.nghost + a.nxp + 1;
     const int wvf_s = a.nghost + 1, wvf_n = a.nghost + a.nyp + 1;
     const size_t ustride = (size_t)(nx + 1) * ny, vstride = (size_t)nx * (ny + 1);
-    const bool on[4] = {I >= 2 && !((a.wall_w && I == wuf_w) || (a.wall_e && I == wuf_e)),
-                        I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e)),
-                        J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n)),
-                        J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))};
+    bool on[4] = {I >= 2 && !((a.wall_w && I == wuf_w) || (a.wall_e && I == wuf_e)),
+                  I <= nx - 1 && !((a.wall_w && I + 1 == wuf_w) || (a.wall_e && I + 1 == wuf_e)),
+                  J >= 2 && !((a.wall_s && J == wvf_s) || (a.wall_n && J == wvf_n)),
+                  J <= ny - 1 && !((a.wall_s && J + 1 == wvf_s) || (a.wall_n && J + 1 == wvf_n))};
     const int fo[4] = {i + (nx + 1) * j, i + 1 + (nx + 1) * j, i + nx * j, i + nx * (j + 1)};
+    // dry faces (inert coefficients, recorded by the sweep) carry only +0.0
+    // fluxes, which the face flux does not store: adding them would leave
+    // every sum unchanged, so the walk skips them
+    if (a.u.dry) {
+        on[0] = on[0] && !a.u.dry[fo[0]];
+        on[1] = on[1] && !a.u.dry[fo[1]];
+    }
+    if (a.v.dry) {
+        on[2] = on[2] && !a.v.dry[fo[2]];
+        on[3] = on[3] && !a.v.dry[fo[3]];
+    }
     const double iaij = 1.0 / LD::ld(a.areaT + col);
     int ptr[4] = {0, 0, 0, 0};
     int bad = 0;

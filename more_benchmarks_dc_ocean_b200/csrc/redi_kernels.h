@@ -53,6 +53,9 @@ struct FaceOutT {
     typename P::Ko* KoL;
     typename P::Ko* KoR;
     typename P::He* hEff;
+    // per face: 1 where the sweep wrote inert coefficients (a dry face: every
+    // flux is +0.0), else 0; may be null (not recorded)
+    uint8_t* dry = nullptr;
 };
 
 template <class P>
@@ -62,6 +65,10 @@ struct FaceInT {
     const typename P::Ko* KoL;
     const typename P::Ko* KoR;
     const typename P::He* hEff;
+    // the sweep's dry-face record (may be null): the face flux stores nothing
+    // for a dry face and the gather skips it, which adds exactly the +0.0
+    // fluxes the face would have had
+    const uint8_t* dry = nullptr;
 };
 
 using FaceOut = FaceOutT<PlainPrec>;
