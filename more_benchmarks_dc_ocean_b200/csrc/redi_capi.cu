@@ -881,6 +881,9 @@ int redi_b200_step_host(const redi_b200_grid* grid, const redi_b200_metrics* met
 // ---------------------------------------------------------------------------
 static std::mutex g_compat_mu;
 static std::vector<Scratch> g_compat_ws;  // one per device
+// the sweep's dry-face record between the two phases of a compat call, one
+// grow-only buffer per device (the phases share g_compat_ws)
+static std::vector<Scratch> g_compat_dry;
 
 static void compat_launch(const char* name, const int* nx_, const int* ny_, const int* nz_, const int* ns_,
                           const double* dt_, const int* nghost_, const int* nxp_, const int* nyp_, const int* ww_,
@@ -913,12 +916,17 @@ static void compat_launch(const char* name, const int* nx_, const int* ny_, cons
     std::lock_guard<std::mutex> lock(g_compat_mu);
     if ((int)g_compat_ws.size() <= dev) g_compat_ws.resize(dev + 1);
     Scratch& ws = g_compat_ws[dev];
+    if ((int)g_compat_dry.size() <= dev) g_compat_dry.resize(dev + 1);
+    Scratch& dry = g_compat_dry[dev];
+    const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
+    if (dry.reserve(nu + nv) != cudaSuccess) { report(REDI_B200_E_NOMEM, "scratch allocation (dry faces)"); return; }
+    uint8_t* udry = static_cast<uint8_t*>(dry.data());
+    uint8_t* vdry = udry + nu;
     cudaStream_t st = 0;  // the reference launches on the legacy default stream
     redi::EosParams e{1, *rho0_, *T_ref_, *S_ref_, *alpha_T_, *beta_S_};  // the launcher's LINEAR EOS
-    redi::FaceOut u{uPoL, uPoR, uKoL, uKoR, uhEff}, v{vPoL, vPoR, vKoL, vKoR, vhEff};
+    redi::FaceOut u{uPoL, uPoR, uKoL, uKoR, uhEff, udry}, v{vPoL, vPoR, vKoL, vKoR, vhEff, vdry};
     int rc = run_phase_a<redi::PlainPrec>(nx, ny, nz, e, h_layer, t_htr, s_htr, wet_u, wet_v, u, v, ws, st);
     if (rc < 0) { report(rc, g_last_error); return; }
-    const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
     cudaMemcpyAsync(khtr_u, khtr_u_ext, nu * 8, cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(khtr_v, khtr_v_ext, nv * 8, cudaMemcpyDeviceToDevice, st);
     PhaseBInputs<redi::PlainPrec> in{};
@@ -926,8 +934,8 @@ static void compat_launch(const char* name, const int* nx_, const int* ny_, cons
     in.walls[0] = *ww_; in.walls[1] = *we_; in.walls[2] = *wsz_; in.walls[3] = *wn_;
     in.dt = *dt_; in.khtr = 0.0; in.khtr_u = khtr_u; in.khtr_v = khtr_v;
     in.dy_cu = dy_cu; in.dx_cv = dx_cv; in.idxCu = idxCu; in.idyCv = idyCv; in.areaT = areaT; in.h = h_layer;
-    in.u = redi::FaceIn{uPoL, uPoR, uKoL, uKoR, uhEff};
-    in.v = redi::FaceIn{vPoL, vPoR, vKoL, vKoR, vhEff};
+    in.u = redi::FaceIn{uPoL, uPoR, uKoL, uKoR, uhEff, udry};
+    in.v = redi::FaceIn{vPoL, vPoR, vKoL, vKoR, vhEff, vdry};
     double* trs[2] = {t_htr, s_htr};
     rc = run_phase_b<redi::PlainPrec>(in, 2, trs, ws, st);
     if (rc < 0) { report(rc, g_last_error); return; }

@@ -120,7 +120,11 @@ int redi_b200_opt_launch_noalloc(const int* nx_, const int* ny_, const int* nz_,
     const size_t fu_b = round256((size_t)2 * (2 * nz + 1) * (size_t)(nx + 1) * ny * sizeof(double));
     const size_t fv_b = round256((size_t)2 * (2 * nz + 1) * (size_t)nx * (ny + 1) * sizeof(double));
     const size_t need_a = ifc_b + pint_b, need_b = ti_b + ppm_b + fu_b + fv_b;
-    const size_t need = need_a > need_b ? need_a : need_b;
+    // the sweep's dry-face record lives behind both phases' scratch (it is
+    // written in Phase A and read in Phase B)
+    const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
+    const size_t dry_off = need_a > need_b ? need_a : need_b;
+    const size_t need = dry_off + round256(nu + nv);
     if (need > kScratchBytes - kHeader)
         return set_error(REDI_B200_E_UNSUPPORTED,
                          "domain needs " + std::to_string(need) + " bytes of scratch; this entry point is limited to " +
@@ -143,8 +147,10 @@ int redi_b200_opt_launch_noalloc(const int* nx_, const int* ny_, const int* nz_,
     redi::SweepArgs sw{};
     sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos.rho0; sw.wet_u = wet_u; sw.wet_v = wet_v;
     sw.ifc = cs.ifc; sw.pint = cs.pint;
-    sw.u = redi::FaceOut{uPoL, uPoR, uKoL, uKoR, uhEff};
-    sw.v = redi::FaceOut{vPoL, vPoR, vKoL, vKoR, vhEff};
+    uint8_t* udry = reinterpret_cast<uint8_t*>(data + dry_off);
+    uint8_t* vdry = udry + nu;
+    sw.u = redi::FaceOut{uPoL, uPoR, uKoL, uKoR, uhEff, udry};
+    sw.v = redi::FaceOut{vPoL, vPoR, vKoL, vKoR, vhEff, vdry};
     if (e == cudaSuccess) e = redi::launch_column_state(cs, st);
     if (e == cudaSuccess) e = redi::launch_sweep<redi::PlainPrec>(sw, st);
     // Per-face diffusivities resolved into the caller's slots (redi_face_copy).
@@ -164,8 +170,8 @@ int redi_b200_opt_launch_noalloc(const int* nx_, const int* ny_, const int* nz_,
     ff.wall_w = *ww_; ff.wall_e = *we_; ff.wall_s = *wsz_; ff.wall_n = *wn_;
     ff.dt = *dt_; ff.khtr = 0.0; ff.khtr_u = khtr_u; ff.khtr_v = khtr_v;
     ff.dy_cu = dy_cu; ff.dx_cv = dx_cv; ff.idxCu = idxCu; ff.idyCv = idyCv;
-    ff.u = redi::FaceIn{uPoL, uPoR, uKoL, uKoR, uhEff};
-    ff.v = redi::FaceIn{vPoL, vPoR, vKoL, vKoR, vhEff};
+    ff.u = redi::FaceIn{uPoL, uPoR, uKoL, uKoR, uhEff, udry};
+    ff.v = redi::FaceIn{vPoL, vPoR, vKoL, vKoR, vhEff, vdry};
     ff.ti = r.ti; ff.ppm = r.ppm;
     ff.Fu = reinterpret_cast<double*>(data + ti_b + ppm_b);
     ff.Fv = reinterpret_cast<double*>(data + ti_b + ppm_b + fu_b);

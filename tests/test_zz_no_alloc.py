@@ -122,7 +122,8 @@ def _need_bytes(nx, ny, nz):
     need_a = r(ncol * (nz + 1) * 32) + r(ncol * (nz + 1) * 8)
     need_b = (r(2 * ncol * (nz + 1) * 8) + r(2 * ncol * nz * 32) + r(2 * (2 * nz + 1) * (nx + 1) * ny * 8)
               + r(2 * (2 * nz + 1) * nx * (ny + 1) * 8))
-    return max(need_a, need_b)
+    dry = r((nx + 1) * ny + nx * (ny + 1))  # the sweep's dry-face record, behind both phases
+    return max(need_a, need_b) + dry
 
 
 def test_noalloc_near_its_limit_at_75_layers():
