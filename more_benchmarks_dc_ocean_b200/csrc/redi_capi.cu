@@ -123,6 +123,7 @@ int run_phase_a(int nx, int ny, int nz, const redi::EosParams& eos, const double
     cs.h = h; cs.th = th; cs.sh = sh;
     cs.ifc = reinterpret_cast<redi::IfcState*>(ws.data());
     cs.pint = reinterpret_cast<double*>(cs.ifc + nifc);
+    cs.wet_u = wet_u; cs.wet_v = wet_v;
     redi::SweepArgsT<P> sw{};
     sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos.rho0;
     sw.wet_u = wet_u; sw.wet_v = wet_v; sw.ifc = cs.ifc; sw.pint = cs.pint;
@@ -164,6 +165,7 @@ int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch&
         rc.ti = reinterpret_cast<double*>(ws.data());
         rc.ppm = reinterpret_cast<typename P::Ppm*>(static_cast<char*>(ws.data()) +
                                                     redi::recon_ppm_offset(in.nx, in.ny, in.nz, nt));
+        rc.dry_u = in.u.dry; rc.dry_v = in.v.dry;
         redi::FaceFluxArgsT<P> ff{};
         ff.nx = in.nx; ff.ny = in.ny; ff.nz = in.nz; ff.ntr = nt;
         ff.nghost = in.nghost; ff.nxp = in.nxp; ff.nyp = in.nyp;

@@ -122,10 +122,27 @@ __device__ __forceinline__ void stream_edges(int nk, Fetch fetch, Emit emit) {
 constexpr int kColumnAhead = 1;
 constexpr int kReconAhead = 1;
 
+// Whether a column is read by the sweep or the face flux: whether any of the
+// faces it borders (u faces i and i+1, v faces j and j+1, where they are
+// interior) passes `wet(face offset)`.
+template <class WetU, class WetV>
+__device__ __forceinline__ bool column_needed(int col, int nx, int ny, WetU wet_u, WetV wet_v) {
+    const int i = col % nx, j = col / nx;
+    return (i >= 1 && wet_u(i + (nx + 1) * j)) || (i + 1 <= nx - 1 && wet_u(i + 1 + (nx + 1) * j)) ||
+           (j >= 1 && wet_v(i + nx * j)) || (j + 1 <= ny - 1 && wet_v(i + nx * (j + 1)));
+}
+
 template <class LD>
 __device__ __forceinline__ void column_state_item(const ColumnStateArgs& a, int col) {
     const int ncol = a.nx * a.ny;
     const int nz = a.nz;
+    if (a.wet_u) {  // the sweep reads a column only for a face with wet > 0 (its inert branch reads nothing)
+        const double* wu = a.wet_u;
+        const double* wv = a.wet_v;
+        if (!column_needed(col, a.nx, a.ny, [wu](int f) { return LD::ld(wu + f) > 0.0; },
+                           [wv](int f) { return LD::ld(wv + f) > 0.0; }))
+            return;
+    }
     const double* __restrict__ h = a.h + col;
     const double* __restrict__ th = a.th + col;
     const double* __restrict__ sh = a.sh + col;
@@ -735,6 +752,12 @@ __device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid, int 
     const int ngroups = (a.ntr + NT - 1) / NT;
     if (gid >= nb * ngroups) return;
     const int col = c0 + gid % nb;
+    if (a.dry_u) {  // the face flux reads a column only for a face that is not dry
+        const uint8_t* du = a.dry_u;
+        const uint8_t* dv = a.dry_v;
+        if (!column_needed(col, a.nx, a.ny, [du](int f) { return du[f] == 0; }, [dv](int f) { return dv[f] == 0; }))
+            return;
+    }
     const int g = gid / nb;
     const int tr0 = g * NT;
     const int nt = min(NT, a.ntr - tr0);

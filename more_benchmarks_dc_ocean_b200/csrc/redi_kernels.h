@@ -82,6 +82,10 @@ struct ColumnStateArgs {
     const double* sh;
     IfcState* ifc;   // [nz+1][column]
     double* pint;    // [nz+1][column]
+    // the sweep's face masks (may be null): a column none of whose sweep faces
+    // is wet is never read by the sweep, and is not computed
+    const double* wet_u = nullptr;
+    const double* wet_v = nullptr;
 };
 
 template <class P>
@@ -103,6 +107,10 @@ struct ReconArgsT {
     const double* htr[kMaxTracers];
     double* ti;               // [tracer][nz+1][column]
     typename P::Ppm* ppm;     // [tracer][nz][column]
+    // the sweep's dry-face record (may be null): a column all of whose faces
+    // are dry is never read by the face flux, and is not reconstructed
+    const uint8_t* dry_u = nullptr;
+    const uint8_t* dry_v = nullptr;
 };
 using ReconArgs = ReconArgsT<PlainPrec>;
 

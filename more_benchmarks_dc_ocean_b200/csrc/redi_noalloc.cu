@@ -144,6 +144,7 @@ int redi_b200_opt_launch_noalloc(const int* nx_, const int* ny_, const int* nz_,
     cs.nx = nx; cs.ny = ny; cs.nz = nz; cs.eos = eos; cs.h = h_layer; cs.th = t_htr; cs.sh = s_htr;
     cs.ifc = reinterpret_cast<redi::IfcState*>(data);
     cs.pint = reinterpret_cast<double*>(data + ifc_b);
+    cs.wet_u = wet_u; cs.wet_v = wet_v;
     redi::SweepArgs sw{};
     sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos.rho0; sw.wet_u = wet_u; sw.wet_v = wet_v;
     sw.ifc = cs.ifc; sw.pint = cs.pint;
@@ -162,6 +163,7 @@ int redi_b200_opt_launch_noalloc(const int* nx_, const int* ny_, const int* nz_,
     r.nx = nx; r.ny = ny; r.nz = nz; r.ntr = 2; r.h = h_layer;
     r.ti = reinterpret_cast<double*>(data);
     r.ppm = reinterpret_cast<redi::PpmLayer*>(data + ti_b);
+    r.dry_u = udry; r.dry_v = vdry;
     r.htr[0] = t_htr;
     r.htr[1] = s_htr;
     redi::FaceFluxArgs ff{};
