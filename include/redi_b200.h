@@ -167,7 +167,13 @@ REDI_B200_API int redi_b200_step_host(const redi_b200_grid* grid, const redi_b20
                                       double dt, const double* khtr_u_ext, const double* khtr_v_ext,
                                       const redi_b200_bc* bc, int nbands, void* stream);
 
-/* Device pointers of the handle's coefficient slots. */
+/* Device pointers of the handle's coefficient slots (FP64 handles). The handle
+ * keeps a record of the faces whose slots hold inert coefficients (dry faces:
+ * redi_calc_coeffs does not rewrite them while they stay dry, and
+ * redi_apply_flux does not walk them); since the caller may write into the
+ * slots through these pointers, this call clears that record (and waits for
+ * the device), so later steps give the reference's results for whatever the
+ * slots then hold. */
 REDI_B200_API int redi_b200_get_coeffs(const redi_b200* self, redi_b200_coeffs* out);
 
 /* Bytes of device scratch the handle holds beside its coefficient slots. */

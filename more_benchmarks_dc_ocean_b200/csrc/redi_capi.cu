@@ -330,18 +330,19 @@ struct redi_b200 {
     void *uKoL = nullptr, *uKoR = nullptr, *vKoL = nullptr, *vKoR = nullptr;
     void *uhEff = nullptr, *vhEff = nullptr;
     double *khtr_u = nullptr, *khtr_v = nullptr;
-    // dry-face record written by the sweep next to the coefficients (0 until
-    // the first redi_calc_coeffs: every face processed)
+    // dry-face record written by the sweep next to the coefficients: 1 at
+    // init (every slot holds the inert coefficients), cleared whenever the
+    // slots are handed out (the caller may write into them)
     uint8_t *udry = nullptr, *vdry = nullptr;
     template <class P>
     redi::FaceOutT<P> out_u() {
         return {uPoL, uPoR, static_cast<typename P::Ko*>(uKoL), static_cast<typename P::Ko*>(uKoR),
-                static_cast<typename P::He*>(uhEff), udry};
+                static_cast<typename P::He*>(uhEff), udry, true};
     }
     template <class P>
     redi::FaceOutT<P> out_v() {
         return {vPoL, vPoR, static_cast<typename P::Ko*>(vKoL), static_cast<typename P::Ko*>(vKoR),
-                static_cast<typename P::He*>(vhEff), vdry};
+                static_cast<typename P::He*>(vhEff), vdry, true};
     }
     template <class P>
     redi::FaceInT<P> in_u() {
@@ -572,8 +573,8 @@ int redi_b200_init(const redi_b200_grid* grid, int nz_ml, int precision, redi_b2
     }
     cudaMemsetAsync(s->khtr_u, 0, nu * 8, st);
     cudaMemsetAsync(s->khtr_v, 0, nv * 8, st);
-    cudaMemsetAsync(s->udry, 0, nu, st);
-    cudaMemsetAsync(s->vdry, 0, nv, st);
+    cudaMemsetAsync(s->udry, 1, nu, st);  // every face holds inert coefficients
+    cudaMemsetAsync(s->vdry, 1, nv, st);
     cudaError_t e2 = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = e2;
     if (e == cudaSuccess) e = cudaGetLastError();
@@ -617,6 +618,14 @@ int redi_b200_get_coeffs(const redi_b200* s, redi_b200_coeffs* out) {
     out->vPoL = s->vPoL; out->vPoR = s->vPoR; out->vhEff = (double*)s->vhEff;
     out->vKoL = (int*)s->vKoL; out->vKoR = (int*)s->vKoR;
     out->khtr_u = s->khtr_u; out->khtr_v = s->khtr_v; out->nsurf = s->nsurf;
+    // The caller may write into the slots: forget which faces hold inert
+    // coefficients, so the next redi_calc_coeffs writes every face again and
+    // redi_apply_flux skips no face it has not seen dry.
+    const size_t nu = (size_t)(s->nx_total + 1) * s->ny_total, nv = (size_t)s->nx_total * (s->ny_total + 1);
+    cudaError_t e = cudaMemset(s->udry, 0, nu);
+    if (e == cudaSuccess) e = cudaMemset(s->vdry, 0, nv);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(e, "redi_b200_get_coeffs");
     return REDI_B200_OK;
 }
 

@@ -351,7 +351,11 @@ __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int 
     Ko* __restrict__ KoR = o.KoR + fo;
     He* __restrict__ hEff = o.hEff + fo;
     const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
-    if (o.dry) o.dry[fo] = wet > 0.0 ? 0 : 1;
+    if (o.dry) {
+        const bool was_dry = o.keep && o.dry[fo];
+        o.dry[fo] = wet > 0.0 ? 0 : 1;
+        if (was_dry && !(wet > 0.0)) return;  // its slots still hold the inert coefficients
+    }
 
     if (!(wet > 0.0)) {  // ocean_redi.F90:722-730: inert coefficients
         for (int s = 0; s < ns; ++s) {
@@ -586,7 +590,11 @@ __device__ __forceinline__ void sweep_item_win(const SweepArgsT<P>& a, int dir, 
     Ko* __restrict__ KoR = o.KoR + fo;
     He* __restrict__ hEff = o.hEff + fo;
     const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
-    if (o.dry) o.dry[fo] = wet > 0.0 ? 0 : 1;
+    if (o.dry) {
+        const bool was_dry = o.keep && o.dry[fo];
+        o.dry[fo] = wet > 0.0 ? 0 : 1;
+        if (was_dry && !(wet > 0.0)) return;  // its slots still hold the inert coefficients
+    }
 
     if (!(wet > 0.0)) {  // ocean_redi.F90:722-730: inert coefficients
         for (int s = 0; s < ns; ++s) {

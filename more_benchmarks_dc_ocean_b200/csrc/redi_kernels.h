@@ -56,6 +56,9 @@ struct FaceOutT {
     // per face: 1 where the sweep wrote inert coefficients (a dry face: every
     // flux is +0.0), else 0; may be null (not recorded)
     uint8_t* dry = nullptr;
+    // the slots are the library's own, and a face recorded dry still holds its
+    // inert coefficients: a face that stays dry is not written again
+    bool keep = false;
 };
 
 template <class P>

@@ -431,3 +431,60 @@ def test_ring_face_flux_edge_cases(redi_lib, oracle_lib, case):
         _compare(_SWEEP_CASES[case](), 2, redi_lib)
     finally:
         autotune.set_flux_staged(saved)
+
+
+def test_dry_faces_follow_changing_masks(redi_lib, oracle_lib):
+    """Faces that turn dry or wet between steps, and slots overwritten by the caller: the handle's
+    record of dry faces (faces whose slots hold inert coefficients are not rewritten, and are not
+    walked by Phase B) follows the masks, and handing out the slots clears it. Coefficients and
+    tracers equal the oracle's after every step."""
+    R = redi_lib
+    p = inputs.make_problem(31, 23, 9, n_seamounts=3, land_fraction=0.3, seed=91)
+    q = p.copy()
+    q.wet_u, q.wet_v = p.wet_u.copy(), p.wet_v.copy()
+    dp = R.to_device(p)
+    redi = R.make_redi(dp)
+    rng = np.random.default_rng(5)
+    c = None
+    for step in range(4):
+        if step in (1, 2):  # flip a tenth of the faces both ways
+            fu = rng.random(q.wet_u.shape) < 0.1
+            fv = rng.random(q.wet_v.shape) < 0.1
+            q.wet_u[fu] = 1.0 - q.wet_u[fu]
+            q.wet_v[fv] = 1.0 - q.wet_v[fv]
+            dp.metrics.wet_u.copy_(torch.from_numpy(q.wet_u))
+            dp.metrics.wet_v.copy_(torch.from_numpy(q.wet_v))
+        if step == 3:  # the caller writes into the slots it was handed (the oracle's too: the
+            # domain-edge faces, which no sweep writes, keep what the caller put there)
+            for k, t in redi.coeffs().items():
+                t.fill_(7)
+                if k in c:
+                    c[k][...] = 7
+        assert R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms) == R.OK
+        assert R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext,
+                                 dp.bc) == R.OK
+        torch.cuda.synchronize()
+        c = O.step(q, 1, coeffs=c)
+        cg = {k: v.cpu().numpy() for k, v in redi.coeffs().items()}
+        for k in ("uPoL", "uPoR", "uKoL", "uKoR", "uhEff", "vPoL", "vPoR", "vKoL", "vKoR", "vhEff"):
+            _assert_exact(f"step {step} {k}", cg[k], c[k])
+        for n, (a, b) in enumerate(zip(dp.ms.tracers, q.tracers)):
+            _assert_exact(f"step {step} tracer {n}", a.cpu().numpy(), b)
+    assert redi.error_count() == 0
+    redi.destroy()
+
+
+def test_apply_flux_before_any_coefficients(redi_lib, oracle_lib):
+    """redi_apply_flux on a fresh handle: every slot holds the inert coefficients of init, so every
+    flux is zero and the tracers come out as the reference's update leaves them."""
+    R = redi_lib
+    p = inputs.make_problem(19, 15, 6, n_seamounts=2, land_fraction=0.2, seed=17)
+    q = p.copy()
+    dp = R.to_device(p)
+    redi = R.make_redi(dp)
+    assert R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc) == R.OK
+    torch.cuda.synchronize()
+    O.apply_flux(q, O.new_coeffs(q.nx, q.ny, q.nz), None, 0)
+    for n, (a, b) in enumerate(zip(dp.ms.tracers, q.tracers)):
+        _assert_exact(f"fresh handle tracer {n}", a.cpu().numpy(), b)
+    redi.destroy()
