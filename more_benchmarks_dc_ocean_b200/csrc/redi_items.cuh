@@ -557,8 +557,68 @@ __device__ __forceinline__ double sw_p(const SweepWin<NR>& r, int side, int q) {
     return r.p[q % NR][side][threadIdx.x];
 }
 
+// Ordered compaction across a block of NT threads: the threads whose `keep`
+// is set write `value` to list[0 .. n) in thread order; returns n. Every
+// thread of the block must call it (two block barriers).
+template <int NT>
+__device__ __forceinline__ int block_compact(bool keep, int value, int* list, int* warp_n) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) warp_n[w] = __popc(m);
+    __syncthreads();
+    int off = 0, total = 0;
+#pragma unroll
+    for (int i = 0; i < NT / 32; ++i) {
+        const int c = warp_n[i];
+        off += i < w ? c : 0;
+        total += c;
+    }
+    if (keep) list[off + __popc(m & ((1u << lane) - 1u))] = value;
+    __syncthreads();
+    return total;
+}
+
+// The part of the sweep for a face that is not wet (ocean_redi.F90:722-730:
+// inert coefficients, and the dry-face record); returns whether face t of
+// direction dir is wet, i.e. whether it needs the sweep.
+template <class P, class LD>
+__device__ __forceinline__ bool sweep_face_dry(const SweepArgsT<P>& a, int dir, int t) {
+    const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
+    int fo;
+    size_t fstride;
+    if (dir == 0) {
+        if (t >= (nx - 1) * ny) return false;
+        fo = 1 + t % (nx - 1) + (nx + 1) * (t / (nx - 1));
+        fstride = (size_t)(nx + 1) * ny;
+    } else {
+        if (t >= nx * (ny - 1)) return false;
+        fo = t % nx + nx * (1 + t / nx);
+        fstride = (size_t)nx * (ny + 1);
+    }
+    const FaceOutT<P> o = dir == 0 ? a.u : a.v;
+    const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
+    if (o.dry) {
+        const bool was_dry = o.keep && o.dry[fo];
+        o.dry[fo] = wet > 0.0 ? 0 : 1;
+        if (was_dry && !(wet > 0.0)) return false;  // its slots still hold the inert coefficients
+    }
+    if (wet > 0.0) return true;
+    using Po = typename P::Po;
+    using Ko = typename P::Ko;
+    using He = typename P::He;
+    for (int s = 0; s < ns; ++s) {
+        o.PoL[fo + s * fstride] = Po(0);
+        o.PoR[fo + s * fstride] = Po(0);
+        o.KoL[fo + s * fstride] = Ko(1);
+        o.KoR[fo + s * fstride] = Ko(1);
+    }
+    for (int s = 0; s < ns - 1; ++s) o.hEff[fo + s * fstride] = He(0);
+    return false;
+}
+
 // r: this block's ring (dynamic shared memory, blocks of kSweepThreads).
-template <class P, class LD, int NR>
+// WET_ONLY: the caller has run sweep_face_dry and t is a wet face.
+template <class P, class LD, int NR, bool WET_ONLY = false>
 __device__ __forceinline__ void sweep_item_win(const SweepArgsT<P>& a, int dir, int t, SweepWin<NR>& r) {
     static_assert(NR >= 3 && NR <= 5, "ring of 3 (none in flight), 4 (one) or 5 (two)");
     const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
@@ -589,22 +649,8 @@ __device__ __forceinline__ void sweep_item_win(const SweepArgsT<P>& a, int dir, 
     Ko* __restrict__ KoL = o.KoL + fo;
     Ko* __restrict__ KoR = o.KoR + fo;
     He* __restrict__ hEff = o.hEff + fo;
-    const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
-    if (o.dry) {
-        const bool was_dry = o.keep && o.dry[fo];
-        o.dry[fo] = wet > 0.0 ? 0 : 1;
-        if (was_dry && !(wet > 0.0)) return;  // its slots still hold the inert coefficients
-    }
-
-    if (!(wet > 0.0)) {  // ocean_redi.F90:722-730: inert coefficients
-        for (int s = 0; s < ns; ++s) {
-            PoL[s * fstride] = Po(0);
-            PoR[s * fstride] = Po(0);
-            KoL[s * fstride] = Ko(1);
-            KoR[s * fstride] = Ko(1);
-        }
-        for (int s = 0; s < ns - 1; ++s) hEff[s * fstride] = He(0);
-        return;
+    if constexpr (!WET_ONLY) {
+        if (!sweep_face_dry<P, LD>(a, dir, t)) return;
     }
 
     const IfcState* XL = a.ifc + colL;
@@ -862,6 +908,23 @@ struct FluxOps<MixedPrec> {
         return (float)dT * he * (float)coef;
     }
 };
+
+// Whether face t of direction dir (t < t_end) is one flux_item computes:
+// an interior face of the launch's range that is neither a wall nor dry.
+template <class P>
+__device__ __forceinline__ bool flux_face_valid(const FaceFluxArgsT<P>& a, int dir, int t, int t_end) {
+    const int nx = a.nx, ny = a.ny;
+    if (dir == 0) {
+        if (!(t < min(t_end, (nx - 1) * ny))) return false;
+        const int j = t / (nx - 1), fi = 1 + t % (nx - 1), I = fi + 1;
+        if ((a.wall_w && I == a.nghost + 1) || (a.wall_e && I == a.nghost + a.nxp + 1)) return false;
+        return !(a.u.dry && a.u.dry[fi + (nx + 1) * j]);
+    }
+    if (!(t < min(t_end, nx * (ny - 1)))) return false;
+    const int fj = 1 + t / nx, i = t % nx, J = fj + 1;
+    if ((a.wall_s && J == a.nghost + 1) || (a.wall_n && J == a.nghost + a.nyp + 1)) return false;
+    return !(a.v.dry && a.v.dry[i + nx * fj]);
+}
 
 // Every lane of the warp must call this (no lane may have exited): lanes
 // without a face of their own (grid tail, wall faces) walk face 0 of their

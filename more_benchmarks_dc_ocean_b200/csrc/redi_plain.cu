@@ -66,12 +66,20 @@ __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgsT<P> a, FaceRang
 
 // The sweep with both windows in a shared-memory ring of NR interfaces per
 // column (dynamic shared memory: sizeof(SweepWin<NR>)).
+// A block's faces are first sorted into dry ones (handled at once) and wet
+// ones, which are compacted onto the block's leading threads in face order, so
+// the sweeps of a block with land run in as few warps as its wet faces fill.
 template <class P, int NR>
 __global__ void __launch_bounds__(kSweepWinThreads) k_neutral_sweep_w(SweepArgsT<P> a, FaceRange r) {
     extern __shared__ __align__(16) unsigned char sweep_win[];
+    __shared__ int list[kSweepWinThreads];
+    __shared__ int warp_n[kSweepWinThreads / 32];
     const int d = blockIdx.x & 1;
     const int t = r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
-    if (t < r.hi[d]) sweep_item_win<P, LdNC, NR>(a, d, t, *reinterpret_cast<SweepWin<NR>*>(sweep_win));
+    const bool wet = t < r.hi[d] && sweep_face_dry<P, LdNC>(a, d, t);
+    const int n = block_compact<kSweepWinThreads>(wet, t, list, warp_n);
+    if ((int)threadIdx.x < n)
+        sweep_item_win<P, LdNC, NR, true>(a, d, list[threadIdx.x], *reinterpret_cast<SweepWin<NR>*>(sweep_win));
 }
 
 template <int NT, class P>
@@ -83,10 +91,17 @@ __global__ void __launch_bounds__(128) k_tracer_recon(ReconArgsT<P> a, int c0, i
 // Blocks alternate between the directions (even: u faces, odd: v faces), so the
 // u and v faces of the same rows are in flight together and the second reads of
 // a column's reconstruction are served from L2 instead of HBM.
+// The block's faces that need a flux (not walls, not dry) are compacted onto
+// its leading threads in face order; the others walk as stand-ins or, in warps
+// with no face left, return at once.
 template <int NT, class P>
 __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0, FaceRange r) {
+    __shared__ int list[128];
+    __shared__ int warp_n[4];
     const int d = blockIdx.x & 1;
-    flux_item<NT, P, LdNC>(a, d, r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x, tr0, r.hi[d]);
+    const int t = r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
+    const int n = block_compact<128>(flux_face_valid(a, d, t, r.hi[d]), t, list, warp_n);
+    flux_item<NT, P, LdNC>(a, d, (int)threadIdx.x < n ? list[threadIdx.x] : r.hi[d], tr0, r.hi[d]);
 }
 
 // The face flux with its reconstruction loads staged one sublayer ahead
