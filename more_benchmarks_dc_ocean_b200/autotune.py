@@ -99,7 +99,8 @@ def fold_shape(precision: int, nz: int, ntracers: int) -> Tuple[int, int]:
 
 
 def set_gather_tracers(n: int, smem: int = 0) -> None:
-    """Tracers one cell-gather launch folds (2 or 4) and where its per-layer sums live: 0 registers,
+    """Tracers one cell-gather launch folds (2, 4, or 8: one gather over two face-flux launches of 4,
+    with shared-memory sums and 4-layer chunks) and where its per-layer sums live: 0 registers,
     1 shared memory, 2 shared memory with 8 sublayers fetched per round trip."""
     from . import ocean_redi as R
 
@@ -168,6 +169,8 @@ def tune_tracer_group(dp, redi, reps: int = 2, stream=None) -> dict:
     ntr = len(dp.ms.tracers)
     smem = get_gather_tracers()[1]
     caps = [(g, n) for g in (2, 4, 8) if g <= max(2, ntr) for n in (2, 4) if n <= g]
+    if ntr > 4:
+        caps.append((4, 8))  # one gather over two face-flux launches of 4
     st = torch.cuda.current_stream() if stream is None else stream
     times = {}
     for g in caps:

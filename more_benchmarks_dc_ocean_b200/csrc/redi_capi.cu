@@ -150,7 +150,7 @@ int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch&
                 const double* const* htr_in = nullptr, redi::Band band = redi::Band{}) {
     const int batch = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
     const size_t recon = redi::recon_bytes<P>(in.nx, in.ny, in.nz, batch);
-    const int group = redi::tracer_group(batch, redi::cell_tuning().group);
+    const int group = redi::flux_slots(batch, redi::cell_tuning());
     const size_t flux = redi::flux_bytes<P>(in.nx, in.ny, in.nz, group);
     cudaError_t e = ws.reserve(recon + flux);
     if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (phase B)");
@@ -402,7 +402,7 @@ int redi_b200_set_tracer_group(int max_group) {
 int redi_b200_get_tracer_group(void) { return redi::cell_tuning().group; }
 
 int redi_b200_set_gather_tracers(int n, int smem) {
-    if (n != 2 && n != 4) return fail(REDI_B200_E_ARG, "redi_b200_set_gather_tracers: n must be 2 or 4");
+    if (n != 2 && n != 4 && n != 8) return fail(REDI_B200_E_ARG, "redi_b200_set_gather_tracers: n must be 2, 4 or 8");
     if (smem < 0 || smem > 2) return fail(REDI_B200_E_ARG, "redi_b200_set_gather_tracers: smem must be 0, 1 or 2");
     redi::CellTuning t = redi::cell_tuning();
     t.gather_tracers = n;
@@ -768,7 +768,7 @@ int step_host_impl(const redi_b200_grid* grid, const redi_b200_metrics* metrics,
     // Scratch for both phases up front: no reallocation while the pipeline runs.
     const int batch = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
     const size_t need_b = redi::recon_bytes<P>(nx, ny, nz, batch) +
-                          redi::flux_bytes<P>(nx, ny, nz, redi::tracer_group(batch, redi::cell_tuning().group));
+                          redi::flux_bytes<P>(nx, ny, nz, redi::flux_slots(batch, redi::cell_tuning()));
     const size_t need_a = redi::phase_a_scratch(nx, ny, nz);
     e = s->ws.reserve(need_a > need_b ? need_a : need_b);
     if (e != cudaSuccess) return cuda_fail(e, "redi_b200_step_host: scratch allocation");

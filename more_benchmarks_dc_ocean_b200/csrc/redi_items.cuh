@@ -994,7 +994,7 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
     const double* const tiR0 = a.ti + (size_t)tr0 * ti_stride + colR;
     const typename P::Ppm* const ppL0 = a.ppm + (size_t)tr0 * pp_stride + colL;
     const typename P::Ppm* const ppR0 = a.ppm + (size_t)tr0 * pp_stride + colR;
-    typename P::Flux* const Fo0 = (dir == 0 ? a.Fu : a.Fv) + fo;
+    typename P::Flux* const Fo0 = (dir == 0 ? a.Fu : a.Fv) + fo + (size_t)a.fslot0 * f_stride;
     auto trc = [nt](int n) { return (size_t)(n < nt ? n : 0); };
 
     // Register rotation: while sublayer s is evaluated, hEff(s+1) and the
@@ -1203,7 +1203,7 @@ __device__ __forceinline__ void flux_item_staged(const FaceFluxArgsT<P>& a, int 
     const double* const tiR0 = a.ti + (size_t)tr0 * ti_stride + colR;
     const typename P::Ppm* const ppL0 = a.ppm + (size_t)tr0 * pp_stride + colL;
     const typename P::Ppm* const ppR0 = a.ppm + (size_t)tr0 * pp_stride + colR;
-    typename P::Flux* const Fo0 = (dir == 0 ? a.Fu : a.Fv) + fo;
+    typename P::Flux* const Fo0 = (dir == 0 ? a.Fu : a.Fv) + fo + (size_t)a.fslot0 * f_stride;
     auto trc = [nt](int n) { return (size_t)(n < nt ? n : 0); };
     auto sti_at = [&](int slot, int n, int w) { return sti + ((size_t)((slot * NT + n) * 8 + w)) * kFluxThreads + tid; };
     auto spp_at = [&](int slot, int n, int side) {
@@ -1419,7 +1419,7 @@ __device__ __forceinline__ void flux_item_ring(const FaceFluxArgsT<P>& a, int di
     const size_t ti_stride = ncol * (nz + 1), pp_stride = ncol * nz, f_stride = (size_t)(ns - 1) * fstride;
     const double* const ti0[2] = {a.ti + (size_t)tr0 * ti_stride + colL, a.ti + (size_t)tr0 * ti_stride + colR};
     const Ppm* const pp0[2] = {a.ppm + (size_t)tr0 * pp_stride + colL, a.ppm + (size_t)tr0 * pp_stride + colR};
-    typename P::Flux* const Fo0 = (dir == 0 ? a.Fu : a.Fv) + fo;
+    typename P::Flux* const Fo0 = (dir == 0 ? a.Fu : a.Fv) + fo + (size_t)a.fslot0 * f_stride;
     auto trc = [nt](int n) { return (size_t)(n < nt ? n : 0); };
     auto pp_at = [&](int layer, int side, int n) {
         return rpp + ((size_t)((((layer & 1) * 2 + side) * NT + n) * kU)) * kFluxThreads + tid;
@@ -1761,7 +1761,7 @@ __device__ __forceinline__ void gather_run_s(const typename P::Flux* const (&F)[
     int s = ptr;
     while (s < ns - 1) {
         int kk[U];
-        double ff[U][NT];
+        typename P::Flux ff[U][NT];  // widened to FP64 where added (exact)
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int su = s + u;
@@ -1769,11 +1769,11 @@ __device__ __forceinline__ void gather_run_s(const typename P::Flux* const (&F)[
                 const size_t so = (size_t)su * stride;
                 kk[u] = (int)LD::ld(KoS + so);
 #pragma unroll
-                for (int n = 0; n < NT; ++n) ff[u][n] = (double)LD::ld(F[n] + so);
+                for (int n = 0; n < NT; ++n) ff[u][n] = LD::ld(F[n] + so);
             } else {
                 kk[u] = 0x7fffffff;
 #pragma unroll
-                for (int n = 0; n < NT; ++n) ff[u][n] = 0.0;
+                for (int n = 0; n < NT; ++n) ff[u][n] = typename P::Flux(0);
             }
         }
         bool stop = false;
@@ -1790,7 +1790,8 @@ __device__ __forceinline__ void gather_run_s(const typename P::Flux* const (&F)[
 #pragma unroll
                     for (int n = 0; n < NT; ++n) {
                         const double v = d[n * kGatherThreads];
-                        d[n * kGatherThreads] = left ? v + ff[u][n] : v - ff[u][n];
+                        const double f = (double)ff[u][n];
+                        d[n * kGatherThreads] = left ? v + f : v - f;
                     }
                 }
             }

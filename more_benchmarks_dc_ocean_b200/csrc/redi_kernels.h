@@ -133,8 +133,9 @@ struct FaceFluxArgsT {
     FaceInT<P> u, v;
     const double* ti;                 // [tracer][nz+1][column]
     const typename P::Ppm* ppm;       // [tracer][nz][column]
-    typename P::Flux* Fu;             // [group tracer][ns-1][(nx+1)*ny]
-    typename P::Flux* Fv;             // [group tracer][ns-1][nx*(ny+1)]
+    typename P::Flux* Fu;             // [slot][ns-1][(nx+1)*ny]
+    typename P::Flux* Fv;             // [slot][ns-1][nx*(ny+1)]
+    int fslot0 = 0;                   // slot of the launch's first tracer
 };
 using FaceFluxArgs = FaceFluxArgsT<PlainPrec>;
 
@@ -228,6 +229,21 @@ struct CellTuning {
 };
 CellTuning cell_tuning();
 void set_cell_tuning(const CellTuning& t);
+
+// Tracers per face-flux launch for ntr tracers under tuning t (the staged
+// face flux holds at most 2 tracers in shared memory, the ring form 4).
+inline int flux_group(int ntr, const CellTuning& t) {
+    const int cap = t.flux_staged == 1 ? 2 : (t.flux_staged == 2 ? 4 : 8);
+    return tracer_group(ntr, t.group < cap ? t.group : cap);
+}
+// Whether one gather folds the fluxes of two face-flux launches of 4 tracers
+// (8 tracers per gather: the shared-memory gather with 4-layer chunks).
+inline bool gather_spans_two(int ntr, const CellTuning& t) {
+    return t.gather_tracers >= 8 && flux_group(ntr, t) == 4 && ntr > 4 && t.gather_smem && t.chunk == 4 &&
+           t.bx * t.by == 128;
+}
+// Slots of the flux buffer Phase B needs for ntr tracers.
+inline int flux_slots(int ntr, const CellTuning& t) { return gather_spans_two(ntr, t) ? 8 : flux_group(ntr, t); }
 
 // Phase B as one fused face-flux + fold pass (redi_fold.cuh) instead of the
 // face-flux / cell-gather pair: enable, tile rows (1 or 2) and tracers per

@@ -285,71 +285,83 @@ static void launch_gather(const CellGatherArgsT<P>& cg, int tr, int slot, const 
     launch_end(K_CELL_UPDATE, st);
 }
 
+// 8 tracers per gather: only the shared-memory sums with 4-layer chunks fit
+// (32 KB); gather_spans_two admits no other shape.
+template <class P>
+static void launch_gather_8(const CellGatherArgsT<P>& cg, int tr, const BandRanges& r, const CellTuning& tune,
+                            dim3 cgrid, dim3 block, cudaStream_t st) {
+    launch_begin(K_CELL_UPDATE, st);
+    if (tune.gather_batch >= 8) plain::k_cell_gather_s<8, 4, P, 8><<<cgrid, block, 0, st>>>(cg, tr, 0, r.j0, r.j1);
+    else plain::k_cell_gather_s<8, 4, P><<<cgrid, block, 0, st>>>(cg, tr, 0, r.j0, r.j1);
+    launch_end(K_CELL_UPDATE, st);
+}
+
+// The face flux of tracers tr0 .. tr0+NT-1 into flux-buffer slots
+// ff.fslot0 .. ff.fslot0+NT-1.
 template <int NT, class P>
-static void launch_flux_gather(const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg, int tr0,
-                               const BandRanges& r, const CellTuning& tune, cudaStream_t st) {
-    const dim3 block(tune.bx, tune.by);
-    const dim3 cgrid((cg.nx + tune.bx - 1) / tune.bx, (r.j1 - r.j0 + tune.by - 1) / tune.by);
+static void launch_flux(const FaceFluxArgsT<P>& ff, int tr0, const BandRanges& r, const CellTuning& tune,
+                        cudaStream_t st) {
     const unsigned nb = face_blocks(r.f);
-    if (nb > 0) {
-        const int kid = P::kMixed ? K_MIXED_FLUX : K_FACE_FLUX;
-        bool done = false;
-        if constexpr (NT <= 4) {
-            if (tune.flux_staged == 2) {
-                static int opted[64] = {};
-                int dev = 0;
-                cudaGetDevice(&dev);
-                const int bytes = (int)plain::FluxRing<NT, P>::bytes;
-                if (dev >= 0 && dev < 64 && !opted[dev]) {
-                    cudaFuncSetAttribute(plain::k_face_flux_r<NT, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         bytes);
-                    opted[dev] = 1;
-                }
-                launch_begin(kid, st);
-                plain::k_face_flux_r<NT, P><<<2 * nb, plain::kFluxThreads, bytes, st>>>(ff, tr0, r.f);
-                launch_end(kid, st);
-                done = true;
+    if (nb == 0) return;
+    const int kid = P::kMixed ? K_MIXED_FLUX : K_FACE_FLUX;
+    if constexpr (NT <= 4) {
+        if (tune.flux_staged == 2) {
+            static int opted[64] = {};
+            int dev = 0;
+            cudaGetDevice(&dev);
+            const int bytes = (int)plain::FluxRing<NT, P>::bytes;
+            if (dev >= 0 && dev < 64 && !opted[dev]) {
+                cudaFuncSetAttribute(plain::k_face_flux_r<NT, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                opted[dev] = 1;
             }
-        }
-        if (done) {
-        } else if constexpr (NT <= 2) {
-            if (tune.flux_staged == 1) {
-                // opt into more than 48 KB of dynamic shared memory once per device
-                static int opted[64] = {};
-                int dev = 0;
-                cudaGetDevice(&dev);
-                const int bytes = (int)plain::FluxStage<NT, P>::bytes;
-                if (dev >= 0 && dev < 64 && !opted[dev]) {
-                    cudaFuncSetAttribute(plain::k_face_flux_s<NT, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         bytes);
-                    opted[dev] = 1;
-                }
-                launch_begin(kid, st);
-                plain::k_face_flux_s<NT, P><<<2 * nb, plain::kFluxThreads, bytes, st>>>(ff, tr0, r.f);
-                launch_end(kid, st);
-            } else {
-                launch_begin(kid, st);
-                plain::k_face_flux<NT, P><<<2 * nb, 128, 0, st>>>(ff, tr0, r.f);
-                launch_end(kid, st);
-            }
-        } else {
             launch_begin(kid, st);
-            plain::k_face_flux<NT, P><<<2 * nb, 128, 0, st>>>(ff, tr0, r.f);
+            plain::k_face_flux_r<NT, P><<<2 * nb, plain::kFluxThreads, bytes, st>>>(ff, tr0, r.f);
             launch_end(kid, st);
+            return;
         }
     }
+    if constexpr (NT <= 2) {
+        if (tune.flux_staged == 1) {
+            // opt into more than 48 KB of dynamic shared memory once per device
+            static int opted[64] = {};
+            int dev = 0;
+            cudaGetDevice(&dev);
+            const int bytes = (int)plain::FluxStage<NT, P>::bytes;
+            if (dev >= 0 && dev < 64 && !opted[dev]) {
+                cudaFuncSetAttribute(plain::k_face_flux_s<NT, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                opted[dev] = 1;
+            }
+            launch_begin(kid, st);
+            plain::k_face_flux_s<NT, P><<<2 * nb, plain::kFluxThreads, bytes, st>>>(ff, tr0, r.f);
+            launch_end(kid, st);
+            return;
+        }
+    }
+    launch_begin(kid, st);
+    plain::k_face_flux<NT, P><<<2 * nb, 128, 0, st>>>(ff, tr0, r.f);
+    launch_end(kid, st);
+}
+
+// The gathers of tracers tr0 .. tr0+NS-1, whose fluxes sit in slots 0 .. NS-1:
+// one launch of 8 tracers (WIDE: the fluxes of two face-flux launches), or
+// launches of 4 or 2 tracers, which read consecutive slots.
+template <int NS, class P, bool WIDE = false>
+static void launch_gathers(const CellGatherArgsT<P>& cg, int tr0, const BandRanges& r, const CellTuning& tune,
+                           cudaStream_t st) {
+    const dim3 block(tune.bx, tune.by);
+    const dim3 cgrid((cg.nx + tune.bx - 1) / tune.bx, (r.j1 - r.j0 + tune.by - 1) / tune.by);
     if (cgrid.y == 0) return;
-    // The gather folds tracer pairs (its per-layer sums live in registers);
-    // a group's pairs read consecutive slots of the flux buffer.
-    // The gather folds tracer pairs or quads (its per-layer sums live in
-    // registers); a group's tracers read consecutive slots of the flux buffer.
-    const int gnt = (tune.gather_tracers >= 4 && NT >= 4) ? 4 : (NT < 2 ? NT : 2);
-    for (int g = 0; g < NT; g += gnt) {
+    if constexpr (WIDE) {
+        launch_gather_8<P>(cg, tr0, r, tune, cgrid, block, st);
+        return;
+    }
+    const int gnt = (tune.gather_tracers >= 4 && NS >= 4) ? 4 : (NS < 2 ? NS : 2);
+    for (int g = 0; g < NS; g += gnt) {
         if (tr0 + g >= cg.ntr) break;
         if (gnt == 4) {
-            launch_gather<(NT >= 4 ? 4 : 1), P>(cg, tr0 + g, g, r, tune, cgrid, block, st);
+            launch_gather<(NS >= 4 ? 4 : 1), P>(cg, tr0 + g, g, r, tune, cgrid, block, st);
         } else {
-            launch_gather<(NT < 2 ? NT : 2), P>(cg, tr0 + g, g, r, tune, cgrid, block, st);
+            launch_gather<(NS < 2 ? NS : 2), P>(cg, tr0 + g, g, r, tune, cgrid, block, st);
         }
     }
 }
@@ -491,16 +503,26 @@ cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, 
         launch_recon<P>(rc, r, st);
     }
     const CellTuning tune = cell_tuning();
-    // the staged face flux holds one or two tracers' reconstruction in shared
-    // memory, the ring form up to four
-    const int cap = tune.flux_staged == 1 ? 2 : (tune.flux_staged == 2 ? 4 : 8);
-    const int group = tracer_group(ff.ntr, tune.group < cap ? tune.group : cap);
+    const int group = flux_group(ff.ntr, tune);
+    if (gather_spans_two(ff.ntr, tune)) {
+        // two face-flux launches of 4 tracers (slots 0-3 and 4-7), one gather of 8
+        for (int tr0 = 0; tr0 < ff.ntr; tr0 += 8) {
+            launch_flux<4, P>(ff, tr0, r, tune, st);
+            if (tr0 + 4 < ff.ntr) {
+                FaceFluxArgsT<P> f2 = ff;
+                f2.fslot0 = 4;
+                launch_flux<4, P>(f2, tr0 + 4, r, tune, st);
+            }
+            launch_gathers<8, P, true>(cg, tr0, r, tune, st);
+        }
+        return cudaGetLastError();
+    }
     for (int tr0 = 0; tr0 < ff.ntr; tr0 += group) {
         switch (group) {
-            case 8: launch_flux_gather<8, P>(ff, cg, tr0, r, tune, st); break;
-            case 4: launch_flux_gather<4, P>(ff, cg, tr0, r, tune, st); break;
-            case 2: launch_flux_gather<2, P>(ff, cg, tr0, r, tune, st); break;
-            default: launch_flux_gather<1, P>(ff, cg, tr0, r, tune, st); break;
+            case 8: launch_flux<8, P>(ff, tr0, r, tune, st); launch_gathers<8, P>(cg, tr0, r, tune, st); break;
+            case 4: launch_flux<4, P>(ff, tr0, r, tune, st); launch_gathers<4, P>(cg, tr0, r, tune, st); break;
+            case 2: launch_flux<2, P>(ff, tr0, r, tune, st); launch_gathers<2, P>(cg, tr0, r, tune, st); break;
+            default: launch_flux<1, P>(ff, tr0, r, tune, st); launch_gathers<1, P>(cg, tr0, r, tune, st); break;
         }
     }
     return cudaGetLastError();

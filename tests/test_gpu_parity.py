@@ -282,10 +282,11 @@ def test_mixed_precision_many_tracers_and_gates(redi_lib, oracle_lib):
 
 
 @pytest.mark.parametrize("gnt,smem,chunk", [(2, 1, 4), (2, 1, 8), (2, 1, 16), (4, 0, 4), (4, 1, 8), (2, 2, 8),
-                                            (2, 2, 16), (4, 2, 4)])
+                                            (2, 2, 16), (4, 2, 4), (8, 1, 4), (8, 2, 4), (8, 1, 8)])
 def test_gather_forms_match_oracle(redi_lib, oracle_lib, gnt, smem, chunk):
-    """The gather folding 2 or 4 tracers per launch, with its per-layer sums in registers or in
-    shared memory: the same additions in the same order, so the oracle's bits."""
+    """The gather folding 2, 4 or 8 tracers per launch (8: two face-flux launches of 4 into one
+    flux buffer; with 8-layer chunks it falls back to 4), with its per-layer sums in registers or
+    in shared memory: the same additions in the same order, so the oracle's bits."""
     from more_benchmarks_dc_ocean_b200 import autotune
 
     saved = (autotune.get_tuning(), autotune.get_gather_tracers(), autotune.get_tracer_group())
@@ -293,7 +294,7 @@ def test_gather_forms_match_oracle(redi_lib, oracle_lib, gnt, smem, chunk):
         autotune.set_tuning(64, 2, chunk)
         autotune.set_gather_tracers(gnt, smem)
         autotune.set_tracer_group(4)
-        p = inputs.make_problem(45, 27, 19, n_passive=5, seed=23)
+        p = inputs.make_problem(45, 27, 19, n_passive=5 if gnt < 8 else 8, seed=23)
         _, tg = _run_gpu(p, 1, redi_lib, check_coeffs=False)
         _, to = _run_oracle(p, 1)
         for n, (a, b) in enumerate(zip(tg, to)):
