@@ -111,10 +111,14 @@ __global__ void __launch_bounds__(128) k_face_flux(FaceFluxArgsT<P> a, int tr0, 
 template <int NT, class P>
 __global__ void __launch_bounds__(kFluxThreads) k_face_flux_r(FaceFluxArgsT<P> a, int tr0, FaceRange r) {
     extern __shared__ __align__(16) unsigned char ring[];
+    __shared__ int list[kFluxThreads];
+    __shared__ int warp_n[kFluxThreads / 32];
     double2* rpp = reinterpret_cast<double2*>(ring);
     double* rti = reinterpret_cast<double*>(ring + FluxRing<NT, P>::pp_units * sizeof(double2));
     const int d = blockIdx.x & 1;
-    flux_item_ring<NT, P>(a, d, r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x, tr0, r.hi[d], rpp, rti);
+    const int t = r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
+    const int n = block_compact<kFluxThreads>(flux_face_valid(a, d, t, r.hi[d]), t, list, warp_n);
+    flux_item_ring<NT, P>(a, d, (int)threadIdx.x < n ? list[threadIdx.x] : r.hi[d], tr0, r.hi[d], rpp, rti);
 }
 
 template <int NT, class P>
