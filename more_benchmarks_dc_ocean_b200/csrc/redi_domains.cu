@@ -371,10 +371,12 @@ int build(redi_b200_batch* b, int n, const redi_b200_domain* dom) {
         if ((long long)(nx + 1) * (ny + 1) * ns >= (1LL << 31))
             return bfail(REDI_B200_E_ARG, "redi_b200_batch_create: domain too large");
         const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1), ncol = (size_t)nx * ny;
-        // coefficient slots (inert initial state is irrelevant: every wet interior face is written each step)
+        // coefficient slots (their initial state is irrelevant: the dry-face
+        // record starts at 0, so the first step writes every interior face) and
+        // the record itself
         const size_t coef_b = up256(nu * ns * 8) * 2 + up256(nv * ns * 8) * 2 + up256(nu * ns * sizeof(Ko)) * 2 +
                               up256(nv * ns * sizeof(Ko)) * 2 + up256(nu * (ns - 1) * sizeof(He)) +
-                              up256(nv * (ns - 1) * sizeof(He));
+                              up256(nv * (ns - 1) * sizeof(He)) + up256(nu) + up256(nv);
         const size_t a_b = redi::phase_a_scratch(nx, ny, nz);
         const size_t rb = redi::recon_bytes<P>(nx, ny, nz, ntr), fb = redi::flux_bytes<P>(nx, ny, nz, 2);
         const size_t scratch = std::max(a_b, up256(rb) + fb);
@@ -389,6 +391,10 @@ int build(redi_b200_batch* b, int n, const redi_b200_domain* dom) {
                             (Ko*)take(nu * ns * sizeof(Ko)), (He*)take(nu * (ns - 1) * sizeof(He))};
         redi::FaceOutT<P> v{(double*)take(nv * ns * 8), (double*)take(nv * ns * 8), (Ko*)take(nv * ns * sizeof(Ko)),
                             (Ko*)take(nv * ns * sizeof(Ko)), (He*)take(nv * (ns - 1) * sizeof(He))};
+        // the batch's own slots: a face that stays dry keeps its inert coefficients
+        u.dry = (uint8_t*)take(nu);
+        v.dry = (uint8_t*)take(nv);
+        u.keep = v.keep = true;
         char* sc = base + coef_b;
         DomainDev<P>& d = hd[k];
         std::memset(&d, 0, sizeof(d));
@@ -398,12 +404,14 @@ int build(redi_b200_batch* b, int n, const redi_b200_domain* dom) {
                                                                   D.eos.alpha_T, D.eos.beta_S},
                                      D.ms.h_layer, th, sh, (redi::IfcState*)sc, nullptr};
         d.cs.pint = (double*)(d.cs.ifc + ncol * (nz + 1));
+        d.cs.wet_u = D.metrics.wet_u; d.cs.wet_v = D.metrics.wet_v;
         d.sw.nx = nx; d.sw.ny = ny; d.sw.nz = nz; d.sw.rho0 = D.eos.rho0;
         d.sw.wet_u = D.metrics.wet_u; d.sw.wet_v = D.metrics.wet_v; d.sw.ifc = d.cs.ifc; d.sw.pint = d.cs.pint;
         d.sw.u = u; d.sw.v = v;
         d.rc.nx = nx; d.rc.ny = ny; d.rc.nz = nz; d.rc.ntr = ntr; d.rc.h = D.ms.h_layer;
         d.rc.ti = (double*)sc;
         d.rc.ppm = (typename P::Ppm*)(sc + redi::recon_ppm_offset(nx, ny, nz, ntr));
+        d.rc.dry_u = u.dry; d.rc.dry_v = v.dry;
         int walls[4] = {1, 1, 1, 1};
         walls[0] = D.bc.west == REDI_B200_OBC_WALL; walls[1] = D.bc.east == REDI_B200_OBC_WALL;
         walls[2] = D.bc.south == REDI_B200_OBC_WALL; walls[3] = D.bc.north == REDI_B200_OBC_WALL;
@@ -412,8 +420,8 @@ int build(redi_b200_batch* b, int n, const redi_b200_domain* dom) {
         ff.nyp = D.grid.ny_phys; ff.wall_w = walls[0]; ff.wall_e = walls[1]; ff.wall_s = walls[2]; ff.wall_n = walls[3];
         ff.dt = D.dt; ff.khtr = 0.0; ff.khtr_u = D.khtr_u_ext; ff.khtr_v = D.khtr_v_ext;
         ff.dy_cu = D.metrics.dy_cu; ff.dx_cv = D.metrics.dx_cv; ff.idxCu = D.metrics.idxCu; ff.idyCv = D.metrics.idyCv;
-        ff.u = redi::FaceInT<P>{u.PoL, u.PoR, u.KoL, u.KoR, u.hEff};
-        ff.v = redi::FaceInT<P>{v.PoL, v.PoR, v.KoL, v.KoR, v.hEff};
+        ff.u = redi::FaceInT<P>{u.PoL, u.PoR, u.KoL, u.KoR, u.hEff, u.dry};
+        ff.v = redi::FaceInT<P>{v.PoL, v.PoR, v.KoL, v.KoR, v.hEff, v.dry};
         ff.ti = d.rc.ti; ff.ppm = d.rc.ppm;
         ff.Fu = (typename P::Flux*)(sc + up256(rb));
         ff.Fv = ff.Fu + (size_t)2 * (2 * nz + 1) * nu;

@@ -352,7 +352,7 @@ __device__ __forceinline__ void sweep_item(const SweepArgsT<P>& a, int dir, int 
     He* __restrict__ hEff = o.hEff + fo;
     const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
     if (o.dry) {
-        const bool was_dry = o.keep && o.dry[fo];
+        const bool was_dry = o.keep && LD::ld(o.dry + fo);
         o.dry[fo] = wet > 0.0 ? 0 : 1;
         if (was_dry && !(wet > 0.0)) return;  // its slots still hold the inert coefficients
     }
@@ -598,7 +598,7 @@ __device__ __forceinline__ bool sweep_face_dry(const SweepArgsT<P>& a, int dir, 
     const FaceOutT<P> o = dir == 0 ? a.u : a.v;
     const double wet = LD::ld((dir == 0 ? a.wet_u : a.wet_v) + fo);
     if (o.dry) {
-        const bool was_dry = o.keep && o.dry[fo];
+        const bool was_dry = o.keep && LD::ld(o.dry + fo);
         o.dry[fo] = wet > 0.0 ? 0 : 1;
         if (was_dry && !(wet > 0.0)) return false;  // its slots still hold the inert coefficients
     }
@@ -809,7 +809,8 @@ __device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid, int 
     if (a.dry_u) {  // the face flux reads a column only for a face that is not dry
         const uint8_t* du = a.dry_u;
         const uint8_t* dv = a.dry_v;
-        if (!column_needed(col, a.nx, a.ny, [du](int f) { return du[f] == 0; }, [dv](int f) { return dv[f] == 0; }))
+        if (!column_needed(col, a.nx, a.ny, [du](int f) { return LD::ld(du + f) == 0; },
+                           [dv](int f) { return LD::ld(dv + f) == 0; }))
             return;
     }
     const int g = gid / nb;
@@ -972,7 +973,7 @@ __device__ __forceinline__ void flux_item(const FaceFluxArgsT<P>& a, int dir, in
     {   // a dry face (inert coefficients) has only +0.0 fluxes: nothing is
         // stored and the gather skips it
         const uint8_t* dry = dir == 0 ? a.u.dry : a.v.dry;
-        if (dry && valid && dry[fo]) valid = false;
+        if (dry && valid && LD::ld(dry + fo)) valid = false;
     }
     if (!__any_sync(0xffffffffu, valid)) return;  // warp-uniform
     const FaceInT<P>& c = dir == 0 ? a.u : a.v;
@@ -1695,12 +1696,12 @@ __device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, 
     // fluxes, which the face flux does not store: adding them would leave
     // every sum unchanged, so the walk skips them
     if (a.u.dry) {
-        on[0] = on[0] && !a.u.dry[fo[0]];
-        on[1] = on[1] && !a.u.dry[fo[1]];
+        on[0] = on[0] && !LD::ld(a.u.dry + fo[0]);
+        on[1] = on[1] && !LD::ld(a.u.dry + fo[1]);
     }
     if (a.v.dry) {
-        on[2] = on[2] && !a.v.dry[fo[2]];
-        on[3] = on[3] && !a.v.dry[fo[3]];
+        on[2] = on[2] && !LD::ld(a.v.dry + fo[2]);
+        on[3] = on[3] && !LD::ld(a.v.dry + fo[3]);
     }
     const double iaij = 1.0 / LD::ld(a.areaT + col);
     int ptr[4] = {0, 0, 0, 0};
@@ -1822,12 +1823,12 @@ __device__ __forceinline__ void gather_item_s(const CellGatherArgsT<P>& a, int i
     // fluxes, which the face flux does not store: adding them would leave
     // every sum unchanged, so the walk skips them
     if (a.u.dry) {
-        on[0] = on[0] && !a.u.dry[fo[0]];
-        on[1] = on[1] && !a.u.dry[fo[1]];
+        on[0] = on[0] && !LD::ld(a.u.dry + fo[0]);
+        on[1] = on[1] && !LD::ld(a.u.dry + fo[1]);
     }
     if (a.v.dry) {
-        on[2] = on[2] && !a.v.dry[fo[2]];
-        on[3] = on[3] && !a.v.dry[fo[3]];
+        on[2] = on[2] && !LD::ld(a.v.dry + fo[2]);
+        on[3] = on[3] && !LD::ld(a.v.dry + fo[3]);
     }
     const double iaij = 1.0 / LD::ld(a.areaT + col);
     int ptr[4] = {0, 0, 0, 0};
