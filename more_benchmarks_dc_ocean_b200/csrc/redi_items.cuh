@@ -561,8 +561,9 @@ __device__ __forceinline__ double sw_p(const SweepWin<NR>& r, int side, int q) {
 // is set write `value` to list[0 .. n) in thread order; returns n. Every
 // thread of the block must call it (two block barriers).
 template <int NT>
-__device__ __forceinline__ int block_compact(bool keep, int value, int* list, int* warp_n) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+__device__ __forceinline__ int block_compact(bool keep, int value, int* list, int* warp_n, int tid = -1) {
+    if (tid < 0) tid = threadIdx.x;  // the thread's linear index in the block
+    const int lane = tid & 31, w = tid >> 5;
     const unsigned m = __ballot_sync(0xffffffffu, keep);
     if (lane == 0) warp_n[w] = __popc(m);
     __syncthreads();
