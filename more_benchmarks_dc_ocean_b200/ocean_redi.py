@@ -306,7 +306,11 @@ class OceanRedi:
 
     # -- coefficient slots (device views) -----------------------------------
     def coeffs(self) -> dict:
-        """uPoL ... vhEff, khtr_u, khtr_v as torch views of the handle's device slots."""
+        """uPoL ... vhEff, khtr_u, khtr_v as torch views of the handle's device slots (FP64 handles).
+
+        The views are writable, so this clears the handle's record of dry faces (faces whose slots
+        hold the inert coefficients): the next redi_calc_coeffs rewrites every face. It waits for
+        the device."""
         import torch
 
         c = _Coeffs()
