@@ -3,7 +3,8 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                     [--config config1|config3|config0|config4] [--precision fp64|mixed]
 
-One step = redi_calc_coeffs + redi_apply_flux over every tracer of the domain.
+One step = redi_calc_coeffs + redi_apply_flux over every tracer of the domain (one redi_b200_step
+call: the same two phases, with the column state and the T/S reconstruction in one pass).
 Metric (the reference's headline): tracer-cell updates/s = N_tracers * nx_phys * ny_phys * nz
 / t_step, land cells included; `value` sums all ranks.
 
@@ -56,7 +57,7 @@ UNIT = "tracer-cell updates/s"
 KERNEL_NAMES = ["k_column_state", "k_neutral_sweep", "k_tracer_recon", "k_cell_gather", "k_face_flux",
                 "k_mixed_recon", "k_mixed_flux", "k_mixed_sweep", "k_domain_persistent", "aux",
                 "k_meke_column", "k_meke_del2", "k_meke_lateral", "k_ale_columns", "k_ale_faces",
-                "k_flux_fold", "k_mixed_fold"]
+                "k_flux_fold", "k_mixed_fold", "k_column_recon"]
 NKERN = len(KERNEL_NAMES)
 FALLBACK_HBM_GBS = 6650.0
 
@@ -119,6 +120,8 @@ def kernel_bytes(p, kid: int, precision: str = "fp64") -> float:
         return float(16 * s["Nt"] * min(2, s["ntr"]) + 8 * s["ncol"])
     if kid in (15, 16):  # fused face flux + fold: the coefficients once, every tracer read + written
         return float(bcoef + face2d + 16 * s["Nt"] * s["ntr"])
+    if kid == 17:        # column state + T/S reconstruction in one pass: read h, T, S once
+        return 24.0 * s["Nt"]
     return 0.0
 
 
@@ -885,8 +888,7 @@ def _e2e(args, p, dp, redi, ex, st, dist, dev, world):
             for d, h in zip(dp.ms.tracers, host_tr):
                 d.copy_(h, non_blocking=True)
             ex.exchange()
-            R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, st)
-            R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, st)
+            R.step(dp, redi, 1, st)
             for d, h in zip(dp.ms.tracers, host_tr):
                 h.copy_(d, non_blocking=True)
 

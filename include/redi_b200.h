@@ -167,6 +167,18 @@ REDI_B200_API int redi_b200_step_host(const redi_b200_grid* grid, const redi_b20
                                       double dt, const double* khtr_u_ext, const double* khtr_v_ext,
                                       const redi_b200_bc* bc, int nbands, void* stream);
 
+/* One whole step: redi_b200_calc_coeffs followed by redi_b200_apply_flux on
+ * the same state, with the same arguments, gates, status and results (bit for
+ * bit). No counterpart in the reference as one routine (its driver calls the
+ * two in turn; its redi_opt_launch does both). Since nothing can change the
+ * tracers between the phases, when tracers 1 and 2 are T and S (either order)
+ * the column state of Phase A and the reconstruction of T and S for Phase B
+ * are computed in one pass over the columns. Stream-ordered on `stream`. */
+REDI_B200_API int redi_b200_step(const redi_b200_grid* grid, const redi_b200_metrics* metrics,
+                                 const redi_b200_eos* eos, redi_b200* self, const redi_b200_state* ms, double dt,
+                                 const double* khtr_u_ext, const double* khtr_v_ext, const redi_b200_bc* bc,
+                                 void* stream);
+
 /* Device pointers of the handle's coefficient slots (FP64 handles). The handle
  * keeps a record of the faces whose slots hold inert coefficients (dry faces:
  * redi_calc_coeffs does not rewrite them while they stay dry, and

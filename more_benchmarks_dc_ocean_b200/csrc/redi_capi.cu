@@ -147,7 +147,7 @@ struct PhaseBInputs {
 // updated ones; band restricts the launches to a band of rows.
 template <class P>
 int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch& ws, cudaStream_t st,
-                const double* const* htr_in = nullptr, redi::Band band = redi::Band{}) {
+                const double* const* htr_in = nullptr, redi::Band band = redi::Band{}, int recon_from = 0) {
     const int batch = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
     const size_t recon = redi::recon_bytes<P>(in.nx, in.ny, in.nz, batch);
     const int group = redi::flux_slots(batch, redi::cell_tuning());
@@ -183,7 +183,7 @@ int run_phase_b(const PhaseBInputs<P>& in, int ntr, double* const* htr, Scratch&
             cg.htr[n] = htr[t0 + n];
             cg.htr_in[n] = htr_in ? htr_in[t0 + n] : htr[t0 + n];
         }
-        e = redi::launch_phase_b<P>(rc, ff, cg, st, band);
+        e = redi::launch_phase_b<P>(rc, ff, cg, st, band, t0 == 0 ? recon_from : 0);
         if (e != cudaSuccess) return cuda_fail(e, "phase B launch");
     }
     return REDI_B200_OK;
@@ -641,8 +641,9 @@ int redi_b200_error_count(const redi_b200* s, int reset) {
     return v;
 }
 
-int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
-                          redi_b200* s, const redi_b200_state* ms, void* stream) {
+// The gates and argument checks of redi_b200_calc_coeffs: OK, SKIPPED or an error.
+static int check_calc(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
+                      redi_b200* s, const redi_b200_state* ms) {
     if (!grid || !metrics || !eos || !s || !ms) return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: NULL argument");
     // Gates of ocean_redi.F90:585-593.
     if (!s->is_init) return REDI_B200_SKIPPED;
@@ -665,6 +666,16 @@ int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* m
         return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: NULL device array");
     if (!aligned(ms->h_layer) || !aligned(th) || !aligned(sh) || !aligned(metrics->wet_u) || !aligned(metrics->wet_v))
         return fail(REDI_B200_E_ARG, "redi_b200_calc_coeffs: misaligned device array");
+    return REDI_B200_OK;
+}
+
+int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
+                          redi_b200* s, const redi_b200_state* ms, void* stream) {
+    const int chk = check_calc(grid, metrics, eos, s, ms);
+    if (chk != REDI_B200_OK) return chk;
+    const int nx = grid->nx_total, ny = grid->ny_total, nz = ms->nz_ml;
+    const double* th = ms->hTr[ms->idx_temperature - 1];
+    const double* sh = ms->hTr[ms->idx_salinity - 1];
     redi::EosParams e{eos->variant, eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (s->precision == REDI_B200_MIXED)
@@ -674,9 +685,11 @@ int redi_b200_calc_coeffs(const redi_b200_grid* grid, const redi_b200_metrics* m
                                         s->out_u<redi::PlainPrec>(), s->out_v<redi::PlainPrec>(), s->ws, st);
 }
 
-int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* metrics, redi_b200* s,
-                         const redi_b200_state* ms, double dt, const double* khtr_u_ext, const double* khtr_v_ext,
-                         const redi_b200_bc* bc, void* stream) {
+// The gates and argument checks of redi_b200_apply_flux: OK, SKIPPED or an
+// error; walls receives the boundary walls.
+static int check_apply(const redi_b200_grid* grid, const redi_b200_metrics* metrics, redi_b200* s,
+                       const redi_b200_state* ms, const double* khtr_u_ext, const double* khtr_v_ext,
+                       const redi_b200_bc* bc, int walls[4]) {
     if (!grid || !metrics || !s || !ms) return fail(REDI_B200_E_ARG, "redi_b200_apply_flux: NULL argument");
     // Gates of ocean_redi.F90:951-959.
     if (!s->is_init) return REDI_B200_SKIPPED;
@@ -688,7 +701,7 @@ int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* me
     if (nx != s->nx_total || ny != s->ny_total)
         return fail(REDI_B200_E_ARG, "redi_b200_apply_flux: grid extents differ from the handle's");
     // ocean_redi.F90:964-973: walls default closed.
-    int walls[4] = {1, 1, 1, 1};
+    walls[0] = walls[1] = walls[2] = walls[3] = 1;
     if (bc) {
         walls[0] = bc->west == REDI_B200_OBC_WALL;
         walls[1] = bc->east == REDI_B200_OBC_WALL;
@@ -703,7 +716,17 @@ int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* me
     for (int t = 0; t < ms->ntracers; ++t)
         if (!ms->hTr[t] || !aligned(ms->hTr[t]))
             return fail(REDI_B200_E_ARG, "redi_b200_apply_flux: NULL or misaligned tracer " + std::to_string(t + 1));
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    return REDI_B200_OK;
+}
+
+// Phase B of a step whose arguments passed check_apply: the per-face KhTr
+// into the slots, then the fluxes of every tracer (recon_from: tracers of the
+// first batch already reconstructed).
+static int run_apply(const redi_b200_grid* grid, const redi_b200_metrics* metrics, redi_b200* s,
+                     const redi_b200_state* ms, double dt, const double* khtr_u_ext, const double* khtr_v_ext,
+                     const int walls[4], cudaStream_t st, int recon_from) {
+    const int nx = grid->nx_total, ny = grid->ny_total, nz = ms->nz_ml;
+    const bool use_ext = khtr_u_ext && khtr_v_ext;
     const size_t nu = (size_t)(nx + 1) * ny, nv = (size_t)nx * (ny + 1);
     // Resolve the per-face KhTr into the slots (:981-987).
     cudaError_t e;
@@ -727,13 +750,96 @@ int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* me
         fill_in(in);
         in.u = s->in_u<redi::MixedPrec>();
         in.v = s->in_v<redi::MixedPrec>();
-        return run_phase_b<redi::MixedPrec>(in, ms->ntracers, ms->hTr, s->ws, st);
+        return run_phase_b<redi::MixedPrec>(in, ms->ntracers, ms->hTr, s->ws, st, nullptr, redi::Band{}, recon_from);
     }
     PhaseBInputs<redi::PlainPrec> in{};
     fill_in(in);
     in.u = s->in_u<redi::PlainPrec>();
     in.v = s->in_v<redi::PlainPrec>();
-    return run_phase_b<redi::PlainPrec>(in, ms->ntracers, ms->hTr, s->ws, st);
+    return run_phase_b<redi::PlainPrec>(in, ms->ntracers, ms->hTr, s->ws, st, nullptr, redi::Band{}, recon_from);
+}
+
+int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* metrics, redi_b200* s,
+                         const redi_b200_state* ms, double dt, const double* khtr_u_ext, const double* khtr_v_ext,
+                         const redi_b200_bc* bc, void* stream) {
+    int walls[4];
+    const int chk = check_apply(grid, metrics, s, ms, khtr_u_ext, khtr_v_ext, bc, walls);
+    if (chk != REDI_B200_OK) return chk;
+    return run_apply(grid, metrics, s, ms, dt, khtr_u_ext, khtr_v_ext, walls, reinterpret_cast<cudaStream_t>(stream), 0);
+}
+
+
+}  // extern "C"
+
+// Phase A of a whole step whose tracers 1 and 2 are T and S (either order):
+// the column state and the reconstruction of T and S in one pass, then the
+// sweep. Phase B's buffers come first in the scratch (as run_phase_b lays them
+// out) and Phase A's behind them, so both live until the fluxes are done.
+template <class P>
+static int run_step_phase_a(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
+                            redi_b200* s, const redi_b200_state* ms, int ts_swap, cudaStream_t st) {
+    const int nx = grid->nx_total, ny = grid->ny_total, nz = ms->nz_ml, ntr = ms->ntracers;
+    const int batch = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
+    const size_t recon = redi::recon_bytes<P>(nx, ny, nz, batch);
+    const size_t flux = redi::flux_bytes<P>(nx, ny, nz, redi::flux_slots(batch, redi::cell_tuning()));
+    const size_t b_end = (recon + flux + 255) & ~size_t(255);
+    cudaError_t e = s->ws.reserve(b_end + redi::phase_a_scratch(nx, ny, nz));
+    if (e != cudaSuccess) return cuda_fail(e, "redi_b200_step: scratch allocation");
+    char* base = static_cast<char*>(s->ws.data());
+    const size_t nifc = (size_t)nx * ny * (nz + 1);
+    redi::ColumnStateArgs cs{};
+    cs.nx = nx; cs.ny = ny; cs.nz = nz;
+    cs.eos = redi::EosParams{eos->variant, eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
+    cs.h = ms->h_layer; cs.th = ms->hTr[ms->idx_temperature - 1]; cs.sh = ms->hTr[ms->idx_salinity - 1];
+    cs.ifc = reinterpret_cast<redi::IfcState*>(base + b_end);
+    cs.pint = reinterpret_cast<double*>(cs.ifc + nifc);
+    cs.wet_u = metrics->wet_u; cs.wet_v = metrics->wet_v;
+    redi::ReconArgsT<P> rc{};
+    rc.nx = nx; rc.ny = ny; rc.nz = nz; rc.ntr = batch; rc.h = ms->h_layer;
+    rc.ti = reinterpret_cast<double*>(base);
+    rc.ppm = reinterpret_cast<typename P::Ppm*>(base + redi::recon_ppm_offset(nx, ny, nz, batch));
+    rc.htr[0] = ms->hTr[0];
+    rc.htr[1] = ms->hTr[1];
+    e = redi::launch_column_recon<P>(cs, rc, ts_swap, st);
+    redi::SweepArgsT<P> sw{};
+    sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos->rho0;
+    sw.wet_u = metrics->wet_u; sw.wet_v = metrics->wet_v; sw.ifc = cs.ifc; sw.pint = cs.pint;
+    sw.u = s->out_u<P>(); sw.v = s->out_v<P>();
+    if (e == cudaSuccess) e = redi::launch_sweep<P>(sw, st);
+    if (e != cudaSuccess) return cuda_fail(e, "redi_b200_step: phase A launch");
+    return REDI_B200_OK;
+}
+
+extern "C" {
+
+int redi_b200_step(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
+                   redi_b200* s, const redi_b200_state* ms, double dt, const double* khtr_u_ext,
+                   const double* khtr_v_ext, const redi_b200_bc* bc, void* stream) {
+    const int ca = check_calc(grid, metrics, eos, s, ms);
+    if (ca < 0) return ca;
+    int walls[4];
+    const int cb = check_apply(grid, metrics, s, ms, khtr_u_ext, khtr_v_ext, bc, walls);
+    if (cb < 0) return cb;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int iT = ms->idx_temperature, iS = ms->idx_salinity;
+    const bool fused = ca == REDI_B200_OK && cb == REDI_B200_OK && ((iT == 1 && iS == 2) || (iT == 2 && iS == 1));
+    if (!fused) {  // the two calls, each with its own gates
+        if (ca == REDI_B200_OK) {
+            const int r = redi_b200_calc_coeffs(grid, metrics, eos, s, ms, stream);
+            if (r < 0) return r;
+        }
+        if (cb == REDI_B200_OK) {
+            const int r = run_apply(grid, metrics, s, ms, dt, khtr_u_ext, khtr_v_ext, walls, st, 0);
+            if (r < 0) return r;
+        }
+        return (ca == REDI_B200_OK || cb == REDI_B200_OK) ? REDI_B200_OK : REDI_B200_SKIPPED;
+    }
+    const int ts_swap = iT == 2 ? 1 : 0;
+    const int ra = s->precision == REDI_B200_MIXED
+                       ? run_step_phase_a<redi::MixedPrec>(grid, metrics, eos, s, ms, ts_swap, st)
+                       : run_step_phase_a<redi::PlainPrec>(grid, metrics, eos, s, ms, ts_swap, st);
+    if (ra < 0) return ra;
+    return run_apply(grid, metrics, s, ms, dt, khtr_u_ext, khtr_v_ext, walls, st, 2);
 }
 
 }  // extern "C"

@@ -856,6 +856,83 @@ __device__ __forceinline__ void recon_item(const ReconArgsT<P>& a, int gid, int 
 }
 
 // ---------------------------------------------------------------------------
+// Phase A's column state and Phase B's reconstruction of T and S in one pass
+// (a whole step in one call: nothing can change the tracers in between).
+// Both passes stream the same top-down PPM edges of hT and hS over the same
+// thicknesses (stream_edges), so one stream feeds both: the EOS state and
+// pressure of every interface (column_state_item) and the interface values and
+// limited PPM layers of tracers 0 and 1 of the reconstruction buffer
+// (recon_item), which are T and S (ts_swap: tracer 0 is S). The values are
+// those of the two passes bit for bit. A column none of whose faces is wet is
+// read by neither the sweep nor the face flux, and is skipped.
+// ---------------------------------------------------------------------------
+template <class P, class LD>
+__device__ __forceinline__ void column_recon_item(const ColumnStateArgs& a, const ReconArgsT<P>& rc, int ts_swap,
+                                                  int col) {
+    const int ncol = a.nx * a.ny;
+    const int nz = a.nz;
+    if (a.wet_u) {
+        const double* wu = a.wet_u;
+        const double* wv = a.wet_v;
+        if (!column_needed(col, a.nx, a.ny, [wu](int f) { return LD::ld(wu + f) > 0.0; },
+                           [wv](int f) { return LD::ld(wv + f) > 0.0; }))
+            return;
+    }
+    const double* __restrict__ h = a.h + col;
+    const double* __restrict__ tr0 = rc.htr[0] + col;
+    const double* __restrict__ tr1 = rc.htr[1] + col;
+    IfcState* __restrict__ ifc = a.ifc + col;
+    double* __restrict__ pint = a.pint + col;
+    double* __restrict__ ti[2] = {rc.ti + col, rc.ti + (size_t)ncol * (nz + 1) + col};
+    typename P::Ppm* __restrict__ ppm[2] = {rc.ppm + col, rc.ppm + (size_t)ncol * nz + col};
+
+    const EosParams eos = a.eos;
+    const bool linear = eos_is_linear(eos.variant);
+    const double dsv_dt = eos.alpha_T / (eos.rho0 * eos.rho0);  // ocean_eos.F90:511
+    const double dsv_ds = -eos.beta_S / (eos.rho0 * eos.rho0);  // ocean_eos.F90:512
+    const double grho = kGravity * eos.rho0;
+    const int iT = ts_swap ? 1 : 0, iS = ts_swap ? 0 : 1;
+    double pres = 0.0;  // interface pressure
+    double h_layer_above = 0.0;
+    double e_prev[2];
+
+    auto fetch = [&](int t, RawLayer<2>& r) {
+        const size_t off = (size_t)(nz - t) * ncol;  // native k = nz+1-t (1-based)
+        r.h = LD::ld(h + off);
+        r.s[0] = LD::ld(tr0 + off);
+        r.s[1] = LD::ld(tr1 + off);
+    };
+    auto emit = [&](int t, const double (&e)[2], const double (&s_above)[2], double h_t) {
+        // column state (column_state_item)
+        if (t >= 2) pres = pres + grho * h_layer_above;
+        const double eT = e[iT], eS = e[iS];
+        double rho_i, sv_t = dsv_dt, sv_s = dsv_ds;
+        if (linear)
+            rho_i = eos.rho0 + eos.beta_S * (eS - eos.S_ref) - eos.alpha_T * (eT - eos.T_ref);
+        else
+            eos::nonlinear_point(eos.variant, eT, eS, pres, rho_i, sv_t, sv_s);
+        double2* q = reinterpret_cast<double2*>(ifc + (size_t)(t - 1) * ncol);
+        q[0] = make_double2(eT, eS);
+        q[1] = make_double2(-(rho_i * rho_i) * sv_t, -(rho_i * rho_i) * sv_s);
+        pint[(size_t)(t - 1) * ncol] = pres;
+        h_layer_above = h_t;
+        // reconstruction (recon_item)
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+            ti[n][(size_t)(t - 1) * ncol] = e[n];
+            if (t >= 2) {
+                double alk = e_prev[n], ark = e[n];
+                const double tlk = s_above[n];
+                ppm_limit(alk, ark, tlk);
+                store_ppm<P>(ppm[n] + (size_t)(t - 2) * ncol, make_ppm_layer(alk, ark, tlk));
+            }
+            e_prev[n] = e[n];
+        }
+    };
+    stream_edges<2, decltype(fetch), decltype(emit), kColumnAhead>(nz, fetch, emit);
+}
+
+// ---------------------------------------------------------------------------
 // Phase B, step 2: the along-neutral flux of every face, computed once
 // (redi_face_flux + redi_sublayer_dT, ocean_redi.F90:893-925, 1037-1092).
 //

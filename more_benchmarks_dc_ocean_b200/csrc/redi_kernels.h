@@ -200,7 +200,8 @@ enum KernelId : int {
     K_ALE_FACES = 14,     // ALE remap: face velocities
     K_FLUX_FOLD = 15,     // Phase B fused face flux + fold (FP64)
     K_MIXED_FOLD = 16,    // Phase B fused face flux + fold (mixed)
-    K_NUM = 17
+    K_COLUMN_RECON = 17,  // column state + T/S reconstruction in one pass (whole-step call)
+    K_NUM = 18
 };
 
 // Sets the message redi_b200_last_error() returns on the calling thread.
@@ -275,13 +276,19 @@ struct Band {
 };
 
 cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st, Band band = Band{});
+// The column state and the reconstruction of rc's tracers 0 and 1 (T and S,
+// or S and T when ts_swap) in one pass over every column.
+template <class P>
+cudaError_t launch_column_recon(const ColumnStateArgs& cs, const ReconArgsT<P>& rc, int ts_swap, cudaStream_t st);
 // Density and dSV/dT, dSV/dS at n points (T, S, p device arrays).
 cudaError_t launch_eos_points(const EosParams& e, int n, const double* T, const double* S, const double* p,
                               double* rho, double* dsv_dt, double* dsv_ds, cudaStream_t st);
 template <class P>
 cudaError_t launch_sweep(const SweepArgsT<P>& sw, cudaStream_t st, Band band = Band{});
 template <class P>
+// recon_from: the first tracer of rc to reconstruct (tracers before it were
+// reconstructed already, by launch_column_recon).
 cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg,
-                           cudaStream_t st, Band band = Band{});
+                           cudaStream_t st, Band band = Band{}, int recon_from = 0);
 
 }  // namespace redi

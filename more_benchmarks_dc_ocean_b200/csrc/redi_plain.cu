@@ -58,6 +58,12 @@ __global__ void __launch_bounds__(128) k_column_state(ColumnStateArgs a, int c0,
 }
 
 template <class P>
+__global__ void __launch_bounds__(128) k_column_recon(ColumnStateArgs a, ReconArgsT<P> rc, int ts_swap, int ncol) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col < ncol) column_recon_item<P, LdNC>(a, rc, ts_swap, col);
+}
+
+template <class P>
 __global__ void __launch_bounds__(128) k_neutral_sweep(SweepArgsT<P> a, FaceRange r) {
     const int d = blockIdx.x & 1;  // blocks alternate between u and v faces, as in k_face_flux
     const int t = r.lo[d] + (int)(blockIdx.x >> 1) * blockDim.x + threadIdx.x;
@@ -214,6 +220,19 @@ cudaError_t launch_column_state(const ColumnStateArgs& cs, cudaStream_t st, Band
     }
     return cudaGetLastError();
 }
+
+template <class P>
+cudaError_t launch_column_recon(const ColumnStateArgs& cs, const ReconArgsT<P>& rc, int ts_swap, cudaStream_t st) {
+    const int ncol = cs.nx * cs.ny;
+    launch_begin(K_COLUMN_RECON, st);
+    plain::k_column_recon<P><<<(ncol + 127) / 128, 128, 0, st>>>(cs, rc, ts_swap, ncol);
+    launch_end(K_COLUMN_RECON, st);
+    return cudaGetLastError();
+}
+template cudaError_t launch_column_recon<PlainPrec>(const ColumnStateArgs&, const ReconArgsT<PlainPrec>&, int,
+                                                    cudaStream_t);
+template cudaError_t launch_column_recon<MixedPrec>(const ColumnStateArgs&, const ReconArgsT<MixedPrec>&, int,
+                                                    cudaStream_t);
 
 cudaError_t launch_eos_points(const EosParams& e, int n, const double* T, const double* S, const double* p,
                               double* rho, double* dsv_dt, double* dsv_ds, cudaStream_t st) {
@@ -468,12 +487,21 @@ FoldShape fold_shape(int nz, int ntr) {
 }
 
 template <class P>
-cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg,
-                           cudaStream_t st, Band band) {
-    const BandRanges r = band_ranges(rc.nx, rc.ny, band);
+cudaError_t launch_phase_b(const ReconArgsT<P>& rc_all, const FaceFluxArgsT<P>& ff, const CellGatherArgsT<P>& cg,
+                           cudaStream_t st, Band band, int recon_from) {
+    const BandRanges r = band_ranges(rc_all.nx, rc_all.ny, band);
+    // the tracers still to reconstruct: rc_all's from recon_from on
+    ReconArgsT<P> rc = rc_all;
+    if (recon_from > 0) {
+        const size_t ncol = (size_t)rc_all.nx * rc_all.ny;
+        rc.ntr = rc_all.ntr > recon_from ? rc_all.ntr - recon_from : 0;
+        for (int n = 0; n < rc.ntr; ++n) rc.htr[n] = rc_all.htr[n + recon_from];
+        rc.ti = rc_all.ti + (size_t)recon_from * ncol * (rc_all.nz + 1);
+        rc.ppm = rc_all.ppm + (size_t)recon_from * ncol * rc_all.nz;
+    }
     const FoldShape fs = fold_shape<P>(rc.nz, ff.ntr);
     if (fs.nt > 0) {
-        if (r.c1 > r.c0) {
+        if (r.c1 > r.c0 && rc.ntr > 0) {
             launch_recon<P>(rc, r, st);
         }
         if (r.j1 <= r.j0) return cudaGetLastError();
@@ -503,7 +531,7 @@ cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, 
         }
     }
     // Reconstruct in groups of two tracers (register window of 2 scalars).
-    if (r.c1 > r.c0) {
+    if (r.c1 > r.c0 && rc.ntr > 0) {
         launch_recon<P>(rc, r, st);
     }
     const CellTuning tune = cell_tuning();
@@ -535,10 +563,10 @@ cudaError_t launch_phase_b(const ReconArgsT<P>& rc, const FaceFluxArgsT<P>& ff, 
 template cudaError_t launch_sweep<PlainPrec>(const SweepArgsT<PlainPrec>&, cudaStream_t, Band);
 template cudaError_t launch_sweep<MixedPrec>(const SweepArgsT<MixedPrec>&, cudaStream_t, Band);
 template cudaError_t launch_phase_b<PlainPrec>(const ReconArgsT<PlainPrec>&, const FaceFluxArgsT<PlainPrec>&,
-                                               const CellGatherArgsT<PlainPrec>&, cudaStream_t, Band);
+                                               const CellGatherArgsT<PlainPrec>&, cudaStream_t, Band, int);
 template FoldShape fold_shape<PlainPrec>(int, int);
 template FoldShape fold_shape<MixedPrec>(int, int);
 template cudaError_t launch_phase_b<MixedPrec>(const ReconArgsT<MixedPrec>&, const FaceFluxArgsT<MixedPrec>&,
-                                               const CellGatherArgsT<MixedPrec>&, cudaStream_t, Band);
+                                               const CellGatherArgsT<MixedPrec>&, cudaStream_t, Band, int);
 
 }  // namespace redi

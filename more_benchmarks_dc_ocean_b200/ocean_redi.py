@@ -94,6 +94,8 @@ def lib() -> C.CDLL:
                                             C.POINTER(_State), vp]
         L.redi_b200_apply_flux.argtypes = [C.POINTER(_Grid), C.POINTER(_Metrics), vp, C.POINTER(_State), C.c_double,
                                            vp, vp, C.POINTER(_BC), vp]
+        L.redi_b200_step.argtypes = [C.POINTER(_Grid), C.POINTER(_Metrics), C.POINTER(_Eos), vp, C.POINTER(_State),
+                                     C.c_double, vp, vp, C.POINTER(_BC), vp]
         L.redi_b200_get_coeffs.argtypes = [vp, C.POINTER(_Coeffs)]
         L.redi_b200_workspace_bytes.argtypes = [vp]
         L.redi_b200_error_count.argtypes = [vp, C.c_int]
@@ -354,6 +356,19 @@ def redi_apply_flux(grid: HGrid, metrics: OceanMetrics, this: OceanRedi, ms: Mul
                                              float(dt), _ptr(khtr_u_ext), _ptr(khtr_v_ext), bcs, _stream(stream)))
 
 
+def redi_step(grid: HGrid, metrics: OceanMetrics, eos: OceanEos, this: OceanRedi, ms: MultilayerState, dt: float,
+              khtr_u_ext=None, khtr_v_ext=None, bc: Optional[OceanBC] = None, stream=None) -> int:
+    """redi_calc_coeffs then redi_apply_flux in one call (redi_b200_step): the same results bit for bit,
+    with Phase A's column state and the reconstruction of T and S in one pass; returns OK or SKIPPED."""
+    if not this.is_init:
+        return SKIPPED
+    st, keep = ms._c()
+    bcs = C.byref(bc._c()) if bc is not None else None
+    return _check(lib().redi_b200_step(C.byref(grid._c()), C.byref(metrics._c()), C.byref(eos._c()), this._h,
+                                       C.byref(st), float(dt), _ptr(khtr_u_ext), _ptr(khtr_v_ext), bcs,
+                                       _stream(stream)))
+
+
 def redi_opt_launch(nx, ny, nz, dt, nghost, nxp, nyp, walls, eos: OceanEos, h_layer, t_htr, s_htr, wet_u, wet_v,
                     coeffs: dict, khtr_u_ext, khtr_v_ext, khtr_u, khtr_v, dy_cu, dx_cv, idxCu, idyCv, areaT,
                     tr_snap=None, symbol: str = "redi_opt_launch") -> None:
@@ -462,10 +477,9 @@ def make_redi(dp: DeviceProblem, precision: int = FP64) -> OceanRedi:
 
 
 def step(dp: DeviceProblem, redi: OceanRedi, nsteps: int = 1, stream=None) -> None:
-    """``nsteps`` Redi steps (Phase A, then Phase B on every tracer), stream-ordered."""
+    """``nsteps`` Redi steps (Phase A, then Phase B on every tracer: redi_step), stream-ordered."""
     for _ in range(nsteps):
-        redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, stream)
-        redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, stream)
+        redi_step(dp.grid, dp.metrics, dp.eos, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext, dp.bc, stream)
 
 
 # ---------------------------------------------------------------------------

@@ -489,3 +489,54 @@ def test_apply_flux_before_any_coefficients(redi_lib, oracle_lib):
     for n, (a, b) in enumerate(zip(dp.ms.tracers, q.tracers)):
         _assert_exact(f"fresh handle tracer {n}", a.cpu().numpy(), b)
     redi.destroy()
+
+
+@pytest.mark.parametrize("case", ["config0", "vanished", "nz1", "nz2", "tie_break", "swapped_ts", "many_tracers"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_whole_step_call_matches_two_calls(redi_lib, oracle_lib, case, precision):
+    """redi_b200_step (one call; Phase A's column state and the T/S reconstruction in one pass)
+    equals redi_calc_coeffs + redi_apply_flux bit for bit over two steps, FP64 and mixed, and the
+    FP64 form equals the oracle."""
+    R = redi_lib
+    if case == "swapped_ts":
+        p = inputs.make_problem(29, 21, 11, n_seamounts=3, land_fraction=0.3, seed=44)
+        p.tracers = [p.tracers[1], p.tracers[0]]
+        p.idx_temperature, p.idx_salinity = p.idx_salinity, p.idx_temperature
+    elif case == "many_tracers":
+        p = inputs.make_problem(31, 19, 13, n_passive=5, land_fraction=0.3, seed=45)
+    else:
+        p = _SWEEP_CASES[case]()
+    out = []
+    for combined in (False, True):
+        dp = R.to_device(p)
+        redi = R.make_redi(dp, R.MIXED if precision else R.FP64)
+        for _ in range(2):
+            if combined:
+                assert R.redi_step(dp.grid, dp.metrics, dp.eos, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext,
+                                   dp.bc) == R.OK
+            else:
+                assert R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms) == R.OK
+                assert R.redi_apply_flux(dp.grid, dp.metrics, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext,
+                                         dp.bc) == R.OK
+        torch.cuda.synchronize()
+        assert redi.error_count() == 0
+        out.append([t.cpu().numpy() for t in dp.ms.tracers])
+        redi.destroy()
+    for n, (a, b) in enumerate(zip(out[1], out[0])):
+        _assert_exact(f"{case} whole-step call tracer {n}", a, b)
+    if not precision:
+        _, to = _run_oracle(p, 2)
+        for n, (a, b) in enumerate(zip(out[1], to)):
+            _assert_exact(f"{case} whole-step call vs oracle tracer {n}", a, b)
+
+
+def test_whole_step_call_gates(redi_lib):
+    """redi_b200_step keeps each phase's gates: a disabled handle is SKIPPED."""
+    R = redi_lib
+    p = inputs.make_problem(12, 10, 5, seed=2)
+    dp = R.to_device(p)
+    redi = R.make_redi(dp)
+    redi.enable = False
+    assert R.redi_step(dp.grid, dp.metrics, dp.eos, redi, dp.ms, dp.dt, dp.khtr_u_ext, dp.khtr_v_ext,
+                       dp.bc) == R.SKIPPED
+    redi.destroy()
