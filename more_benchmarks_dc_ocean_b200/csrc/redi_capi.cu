@@ -774,40 +774,50 @@ int redi_b200_apply_flux(const redi_b200_grid* grid, const redi_b200_metrics* me
 // Phase A of a whole step whose tracers 1 and 2 are T and S (either order):
 // the column state and the reconstruction of T and S in one pass, then the
 // sweep. Phase B's buffers come first in the scratch (as run_phase_b lays them
-// out) and Phase A's behind them, so both live until the fluxes are done.
+// out for ntr tracers) and Phase A's behind them, so both live until the
+// fluxes are done; run_phase_b with recon_from = 2 follows.
 template <class P>
-static int run_step_phase_a(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
-                            redi_b200* s, const redi_b200_state* ms, int ts_swap, cudaStream_t st) {
-    const int nx = grid->nx_total, ny = grid->ny_total, nz = ms->nz_ml, ntr = ms->ntracers;
+static int run_fused_phase_a(int nx, int ny, int nz, int ntr, const redi::EosParams& eos, const double* h,
+                             const double* tr0, const double* tr1, int ts_swap, const double* wet_u,
+                             const double* wet_v, const redi::FaceOutT<P>& u, const redi::FaceOutT<P>& v,
+                             Scratch& ws, cudaStream_t st) {
     const int batch = ntr < redi::kMaxTracers ? ntr : redi::kMaxTracers;
     const size_t recon = redi::recon_bytes<P>(nx, ny, nz, batch);
     const size_t flux = redi::flux_bytes<P>(nx, ny, nz, redi::flux_slots(batch, redi::cell_tuning()));
     const size_t b_end = (recon + flux + 255) & ~size_t(255);
-    cudaError_t e = s->ws.reserve(b_end + redi::phase_a_scratch(nx, ny, nz));
-    if (e != cudaSuccess) return cuda_fail(e, "redi_b200_step: scratch allocation");
-    char* base = static_cast<char*>(s->ws.data());
+    cudaError_t e = ws.reserve(b_end + redi::phase_a_scratch(nx, ny, nz));
+    if (e != cudaSuccess) return cuda_fail(e, "scratch allocation (whole step)");
+    char* base = static_cast<char*>(ws.data());
     const size_t nifc = (size_t)nx * ny * (nz + 1);
     redi::ColumnStateArgs cs{};
-    cs.nx = nx; cs.ny = ny; cs.nz = nz;
-    cs.eos = redi::EosParams{eos->variant, eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
-    cs.h = ms->h_layer; cs.th = ms->hTr[ms->idx_temperature - 1]; cs.sh = ms->hTr[ms->idx_salinity - 1];
+    cs.nx = nx; cs.ny = ny; cs.nz = nz; cs.eos = eos;
+    cs.h = h; cs.th = ts_swap ? tr1 : tr0; cs.sh = ts_swap ? tr0 : tr1;
     cs.ifc = reinterpret_cast<redi::IfcState*>(base + b_end);
     cs.pint = reinterpret_cast<double*>(cs.ifc + nifc);
-    cs.wet_u = metrics->wet_u; cs.wet_v = metrics->wet_v;
+    cs.wet_u = wet_u; cs.wet_v = wet_v;
     redi::ReconArgsT<P> rc{};
-    rc.nx = nx; rc.ny = ny; rc.nz = nz; rc.ntr = batch; rc.h = ms->h_layer;
+    rc.nx = nx; rc.ny = ny; rc.nz = nz; rc.ntr = batch; rc.h = h;
     rc.ti = reinterpret_cast<double*>(base);
     rc.ppm = reinterpret_cast<typename P::Ppm*>(base + redi::recon_ppm_offset(nx, ny, nz, batch));
-    rc.htr[0] = ms->hTr[0];
-    rc.htr[1] = ms->hTr[1];
+    rc.htr[0] = tr0;
+    rc.htr[1] = tr1;
     e = redi::launch_column_recon<P>(cs, rc, ts_swap, st);
     redi::SweepArgsT<P> sw{};
-    sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos->rho0;
-    sw.wet_u = metrics->wet_u; sw.wet_v = metrics->wet_v; sw.ifc = cs.ifc; sw.pint = cs.pint;
-    sw.u = s->out_u<P>(); sw.v = s->out_v<P>();
+    sw.nx = nx; sw.ny = ny; sw.nz = nz; sw.rho0 = eos.rho0;
+    sw.wet_u = wet_u; sw.wet_v = wet_v; sw.ifc = cs.ifc; sw.pint = cs.pint;
+    sw.u = u; sw.v = v;
     if (e == cudaSuccess) e = redi::launch_sweep<P>(sw, st);
-    if (e != cudaSuccess) return cuda_fail(e, "redi_b200_step: phase A launch");
+    if (e != cudaSuccess) return cuda_fail(e, "phase A launch (whole step)");
     return REDI_B200_OK;
+}
+
+template <class P>
+static int run_step_phase_a(const redi_b200_grid* grid, const redi_b200_metrics* metrics, const redi_b200_eos* eos,
+                            redi_b200* s, const redi_b200_state* ms, int ts_swap, cudaStream_t st) {
+    const redi::EosParams e{eos->variant, eos->rho0, eos->T_ref, eos->S_ref, eos->alpha_T, eos->beta_S};
+    return run_fused_phase_a<P>(grid->nx_total, grid->ny_total, ms->nz_ml, ms->ntracers, e, ms->h_layer, ms->hTr[0],
+                                ms->hTr[1], ts_swap, metrics->wet_u, metrics->wet_v, s->out_u<P>(), s->out_v<P>(),
+                                s->ws, st);
 }
 
 extern "C" {
@@ -1042,7 +1052,8 @@ static void compat_launch(const char* name, const int* nx_, const int* ny_, cons
     cudaStream_t st = 0;  // the reference launches on the legacy default stream
     redi::EosParams e{1, *rho0_, *T_ref_, *S_ref_, *alpha_T_, *beta_S_};  // the launcher's LINEAR EOS
     redi::FaceOut u{uPoL, uPoR, uKoL, uKoR, uhEff, udry}, v{vPoL, vPoR, vKoL, vKoR, vhEff, vdry};
-    int rc = run_phase_a<redi::PlainPrec>(nx, ny, nz, e, h_layer, t_htr, s_htr, wet_u, wet_v, u, v, ws, st);
+    // both phases in this call: the column state and the T/S reconstruction in one pass
+    int rc = run_fused_phase_a<redi::PlainPrec>(nx, ny, nz, 2, e, h_layer, t_htr, s_htr, 0, wet_u, wet_v, u, v, ws, st);
     if (rc < 0) { report(rc, g_last_error); return; }
     cudaMemcpyAsync(khtr_u, khtr_u_ext, nu * 8, cudaMemcpyDeviceToDevice, st);
     cudaMemcpyAsync(khtr_v, khtr_v_ext, nv * 8, cudaMemcpyDeviceToDevice, st);
@@ -1054,7 +1065,7 @@ static void compat_launch(const char* name, const int* nx_, const int* ny_, cons
     in.u = redi::FaceIn{uPoL, uPoR, uKoL, uKoR, uhEff, udry};
     in.v = redi::FaceIn{vPoL, vPoR, vKoL, vKoR, vhEff, vdry};
     double* trs[2] = {t_htr, s_htr};
-    rc = run_phase_b<redi::PlainPrec>(in, 2, trs, ws, st);
+    rc = run_phase_b<redi::PlainPrec>(in, 2, trs, ws, st, nullptr, redi::Band{}, 2);
     if (rc < 0) { report(rc, g_last_error); return; }
     cudaDeviceSynchronize();
 }
