@@ -68,7 +68,7 @@ module redi_b200_c
    end type redi_b200_coeffs
 
    public :: redi_b200_init, redi_b200_destroy, redi_b200_set_enable, redi_b200_set_khtr
-   public :: redi_b200_calc_coeffs, redi_b200_apply_flux, redi_b200_get_coeffs
+   public :: redi_b200_calc_coeffs, redi_b200_apply_flux, redi_b200_step, redi_b200_get_coeffs
    public :: redi_b200_error_count, redi_b200_last_error
 
    interface
@@ -125,6 +125,23 @@ module redi_b200_c
          type(redi_b200_bc), intent(in), optional :: bc ! absent (NULL): every edge a wall
          type(c_ptr), value :: stream
       end function redi_b200_apply_flux
+
+      !> redi_calc_coeffs then redi_apply_flux on the same state, in one call
+      !> (same gates, statuses and results; one column pass fewer)
+      integer(c_int) function redi_b200_step(grid, metrics, eos, h, ms, dt, khtr_u_ext, khtr_v_ext, bc, stream) &
+         bind(C, name="redi_b200_step")
+         import :: c_int, c_ptr, c_double, redi_b200_grid, redi_b200_metrics, redi_b200_eos, redi_b200_state, &
+                   redi_b200_bc
+         type(redi_b200_grid), intent(in) :: grid
+         type(redi_b200_metrics), intent(in) :: metrics
+         type(redi_b200_eos), intent(in) :: eos
+         type(c_ptr), value :: h
+         type(redi_b200_state), intent(in) :: ms
+         real(c_double), value :: dt
+         type(c_ptr), value :: khtr_u_ext, khtr_v_ext
+         type(redi_b200_bc), intent(in), optional :: bc
+         type(c_ptr), value :: stream
+      end function redi_b200_step
 
       !> device addresses of the handle's coefficient slots
       integer(c_int) function redi_b200_get_coeffs(h, out) bind(C, name="redi_b200_get_coeffs")
