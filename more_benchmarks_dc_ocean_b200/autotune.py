@@ -287,7 +287,7 @@ def tune_batch(batch, candidates: Optional[Iterable[Tuple[int, int, int]]] = Non
     """Time whole batch steps for every (bx, by, chunk, occupancy) candidate and keep the fastest.
 
     The persistent kernel runs every stage of every domain, so the candidate is
-    judged on the full step (its tracers are advanced in place). Returns
+    compared on the full step (its tracers are advanced in place). Returns
     {"best": (bx, by, chunk, occupancy), "ms": {candidate: ms per step}}.
     """
     import torch

@@ -77,7 +77,7 @@ def test_config0_one_step(redi_lib, oracle_lib):
 
 
 def test_config0_ten_steps(redi_lib, oracle_lib):
-    """Config 0 as BASELINE.json states it: 10 steps compared against the FP64 oracle."""
+    """Config 0 (128x96x25): 10 steps compared against the FP64 oracle."""
     _compare(inputs.config0(), 10, redi_lib)
 
 
