@@ -468,7 +468,8 @@ def run_b200(args, rank, world, local_rank):
             "clocks": clk,
             "gpu_launches": int(n1 - n0),
             "tuning": {"cell_update_tile": list(tuning["best"][:2]), "vertical_chunk": tuning["best"][2],
-                       "gather_sums": {0: "registers", 1: "shared memory", 2: "shared memory, 8-deep batches"}[
+                       "gather_sums": {0: "registers", 1: "shared memory", 2: "shared memory, 8-deep batches",
+                                       3: "shared memory, pipelined batches of 4"}[
                            tuning["best"][3] if len(tuning["best"]) > 3 else 0],
                        "tracer_group": tuning.get("tracer_group"),
                        "candidates_ms": tuning["ms"]} if tuning else None,
@@ -523,7 +524,8 @@ def _mixed_batched(args, p, dp, st, plain_value: float) -> dict:
     # The FP64 line's gather shape is not the mixed one's best (FP32 fluxes halve the gather's
     # loads), so the mixed step picks its own among the shapes that win in either precision.
     shape2 = autotune.tune(dp, redi, candidates=[(64, 2, 4, 1), (64, 2, 8, 1), (32, 4, 8, 1), (32, 4, 16, 2),
-                                                   (64, 2, 16, 2)], reps=1, use_cache=False, stream=st)
+                                                   (64, 2, 16, 2), (64, 2, 16, 3), (32, 4, 8, 3)], reps=1,
+                           use_cache=False, stream=st)
     ms = _time_steps(dp, redi, st, warm, steps)
     redi.destroy()
     upd = p.ntr * p.nx_phys * p.ny_phys * p.nz / (ms * 1e-3)
@@ -536,7 +538,8 @@ def _mixed_batched(args, p, dp, st, plain_value: float) -> dict:
     dq = R.to_device(q, torch.device("cuda", torch.cuda.current_device()))
     redi = R.make_redi(dq, R.MIXED)
     shape = autotune.tune(dq, redi, candidates=[(64, 2, 4, 0), (64, 2, 4, 1), (32, 4, 4, 1), (64, 2, 8, 1),
-                                                  (32, 4, 8, 1), (32, 4, 4, 2), (32, 4, 8, 2)], reps=1,
+                                                  (32, 4, 8, 1), (32, 4, 4, 2), (32, 4, 8, 2), (32, 4, 8, 3),
+                                                  (64, 2, 8, 3), (32, 4, 4, 3)], reps=1,
                           use_cache=False, stream=st)
     group = autotune.tune_tracer_group(dq, redi, stream=st)
     ms = _time_steps(dq, redi, st, warm, steps)

@@ -240,8 +240,10 @@ REDI_B200_API int redi_b200_get_tracer_group(void);
 /* Tracers one cell-gather launch folds (2, 4 or 8; default 2) and where it
  * keeps a chunk's per-layer sums (smem = 1, the default: the thread's slots in
  * shared memory, one load-add-store per flux; 2: the same, fetching 8
- * sublayers per round trip instead of 3 or 4; 0: registers, a select-add over
- * the chunk), process-wide (no counterpart in the reference). 4 tracers read
+ * sublayers per round trip instead of 3 or 4; 3: the same with batches of 4
+ * software-pipelined, the next batch in flight while one is folded; 0:
+ * registers, a select-add over the chunk), process-wide (no counterpart in the
+ * reference). 4 tracers read
  * the cell-side Ko half as often as 2. 8 folds the fluxes of two face-flux
  * launches of 4 tracers in one walk; it applies with face-flux groups of 4,
  * shared-memory sums, 4-layer chunks and 128-thread tiles (else 4 is used).

@@ -101,7 +101,8 @@ def fold_shape(precision: int, nz: int, ntracers: int) -> Tuple[int, int]:
 def set_gather_tracers(n: int, smem: int = 0) -> None:
     """Tracers one cell-gather launch folds (2, 4, or 8: one gather over two face-flux launches of 4,
     with shared-memory sums and 4-layer chunks) and where its per-layer sums live: 0 registers,
-    1 shared memory, 2 shared memory with 8 sublayers fetched per round trip."""
+    1 shared memory, 2 shared memory with 8 sublayers fetched per round trip, 3 shared memory with
+    batches of 4 software-pipelined (the next batch in flight while one is folded)."""
     from . import ocean_redi as R
 
     L = R.lib()
@@ -237,7 +238,7 @@ def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, ...]]] = None, reps:
     """Time the cell update for every (bx, by, chunk[, smem]) candidate and keep the fastest.
 
     smem = 1 runs the gather with its per-layer sums in shared memory (128-thread tiles), 2 the same
-    with 8 sublayers fetched per round trip.
+    with 8 sublayers fetched per round trip, 3 with batches of 4 software-pipelined.
     Runs redi_apply_flux on ``dp`` (its tracers are advanced in place). Returns
     {"best": (bx, by, chunk, smem), "ms": {candidate: ms per launch}, "cached": bool}.
     """
@@ -254,7 +255,7 @@ def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, ...]]] = None, reps:
     L = _bind(R.lib())
     cands = list(candidates) if candidates is not None else (
         [(bx, by, c, 0) for (bx, by) in TILES for c in CHUNKS] +
-        [(bx, by, c, m) for (bx, by) in SMEM_TILES for c in CHUNKS for m in (1, 2)])
+        [(bx, by, c, m) for (bx, by) in SMEM_TILES for c in CHUNKS for m in (1, 2, 3)])
     R.redi_calc_coeffs(dp.grid, dp.metrics, dp.eos, redi, dp.ms, stream)
     times = {}
     for cand in cands:
@@ -272,7 +273,7 @@ def tune(dp, redi, candidates: Optional[Iterable[Tuple[int, ...]]] = None, reps:
     best = min(times, key=times.get)
     _apply(best)
     _store(dp, prec, best)
-    return {"best": best, "ms": {f"{k[0]}x{k[1]}/ch{k[2]}" + ({1: "/smem", 2: "/smem/u8"}.get(k[3], "") if len(k) > 3 else ""): round(v, 4)
+    return {"best": best, "ms": {f"{k[0]}x{k[1]}/ch{k[2]}" + ({1: "/smem", 2: "/smem/u8", 3: "/smem/pipe"}.get(k[3], "") if len(k) > 3 else ""): round(v, 4)
                                  for k, v in times.items()}, "cached": False}
 
 

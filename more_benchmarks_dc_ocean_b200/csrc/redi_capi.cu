@@ -403,11 +403,12 @@ int redi_b200_get_tracer_group(void) { return redi::cell_tuning().group; }
 
 int redi_b200_set_gather_tracers(int n, int smem) {
     if (n != 2 && n != 4 && n != 8) return fail(REDI_B200_E_ARG, "redi_b200_set_gather_tracers: n must be 2, 4 or 8");
-    if (smem < 0 || smem > 2) return fail(REDI_B200_E_ARG, "redi_b200_set_gather_tracers: smem must be 0, 1 or 2");
+    if (smem < 0 || smem > 3) return fail(REDI_B200_E_ARG, "redi_b200_set_gather_tracers: smem must be 0, 1, 2 or 3");
     redi::CellTuning t = redi::cell_tuning();
     t.gather_tracers = n;
     t.gather_smem = smem ? 1 : 0;
     t.gather_batch = smem == 2 ? 8 : 0;
+    t.gather_pipe = smem == 3 ? 1 : 0;
     redi::set_cell_tuning(t);
     return REDI_B200_OK;
 }
@@ -435,7 +436,8 @@ int redi_b200_get_sweep_form(void) { return redi::cell_tuning().sweep_form; }
 
 
 int redi_b200_get_gather_tracers(int* smem) {
-    if (smem) *smem = redi::cell_tuning().gather_smem ? (redi::cell_tuning().gather_batch >= 8 ? 2 : 1) : 0;
+    const redi::CellTuning t = redi::cell_tuning();
+    if (smem) *smem = t.gather_smem ? (t.gather_pipe ? 3 : (t.gather_batch >= 8 ? 2 : 1)) : 0;
     return redi::cell_tuning().gather_tracers;
 }
 

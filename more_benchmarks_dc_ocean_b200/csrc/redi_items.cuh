@@ -1833,6 +1833,76 @@ __device__ __forceinline__ void gather_item(const CellGatherArgsT<P>& a, int i, 
 // their order are exactly those of gather_run.
 constexpr int kGatherThreads = 128;
 
+// The walk with its batches software-pipelined: the batch after the current
+// one is requested before the current one is folded, so one face's round
+// trips overlap instead of following one another. A batch past the face's
+// stop is fetched in vain (those sublayers belong to the next chunk; their
+// lines are read again there). The additions and their order are exactly those
+// of gather_run_s.
+template <int NT, class P, class LD, int U>
+__device__ __forceinline__ void gather_batch_ld(const typename P::Flux* const (&F)[NT],
+                                                const typename P::Ko* __restrict__ KoS, size_t stride, int ns, int s0,
+                                                int (&kk)[U], typename P::Flux (&ff)[U][NT]) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int su = s0 + u;
+        if (su < ns - 1) {
+            const size_t so = (size_t)su * stride;
+            kk[u] = (int)LD::ld(KoS + so);
+#pragma unroll
+            for (int n = 0; n < NT; ++n) ff[u][n] = LD::ld(F[n] + so);
+        } else {
+            kk[u] = 0x7fffffff;
+#pragma unroll
+            for (int n = 0; n < NT; ++n) ff[u][n] = typename P::Flux(0);
+        }
+    }
+}
+
+template <int NT, int CH, class P, class LD, int U>
+__device__ __forceinline__ void gather_run_sp(const typename P::Flux* const (&F)[NT],
+                                              const typename P::Ko* __restrict__ KoS, size_t stride, bool left, int ns,
+                                              int& ptr, int k0, int k1, double* __restrict__ acc, int& bad) {
+    int s = ptr;
+    if (s >= ns - 1) return;
+    int kk[U];
+    typename P::Flux ff[U][NT];
+    gather_batch_ld<NT, P, LD, U>(F, KoS, stride, ns, s, kk, ff);
+    while (true) {
+        int kn[U];
+        typename P::Flux fn[U][NT];
+        gather_batch_ld<NT, P, LD, U>(F, KoS, stride, ns, s + U, kn, fn);
+        bool stop = false;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = kk[u];
+            stop = stop || k >= k1;  // also the end of the face (s >= ns-1)
+            if (!stop) {
+                ++s;
+                if (k < k0) {
+                    ++bad;
+                } else {
+                    double* d = acc + (size_t)(k - k0) * NT * kGatherThreads;
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) {
+                        const double v = d[n * kGatherThreads];
+                        const double f = (double)ff[u][n];
+                        d[n * kGatherThreads] = left ? v + f : v - f;
+                    }
+                }
+            }
+        }
+        if (stop) break;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            kk[u] = kn[u];
+#pragma unroll
+            for (int n = 0; n < NT; ++n) ff[u][n] = fn[u][n];
+        }
+    }
+    ptr = s;
+}
+
 template <int NT, int CH, class P, class LD, int U = 4>
 __device__ __forceinline__ void gather_run_s(const typename P::Flux* const (&F)[NT],
                                              const typename P::Ko* __restrict__ KoS, size_t stride, bool left, int ns,
@@ -1880,7 +1950,7 @@ __device__ __forceinline__ void gather_run_s(const typename P::Flux* const (&F)[
     ptr = s;
 }
 
-template <int NT, int CH, class P, class LD, int U = 4>
+template <int NT, int CH, class P, class LD, int U = 4, bool PIPE = false>
 __device__ __forceinline__ void gather_item_s(const CellGatherArgsT<P>& a, int i, int j, int tr0, int fslot,
                                               double* __restrict__ acc) {
     const int nx = a.nx, ny = a.ny, nz = a.nz, ns = 2 * nz + 2;
@@ -1925,8 +1995,12 @@ __device__ __forceinline__ void gather_item_s(const CellGatherArgsT<P>& a, int i
             for (int n = 0; n < NT; ++n)
                 F[n] = (u ? a.Fu : a.Fv) + (size_t)(fslot + (n < nt ? n : 0)) * (size_t)(ns - 1) * stride + fo[f];
             const FaceInT<P>& c = u ? a.u : a.v;
-            gather_run_s<NT, CH, P, LD, U>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1, acc,
-                                           bad);
+            if constexpr (PIPE)
+                gather_run_sp<NT, CH, P, LD, U>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1,
+                                                acc, bad);
+            else
+                gather_run_s<NT, CH, P, LD, U>(F, (left ? c.KoL : c.KoR) + fo[f], stride, left, ns, ptr[f], k0, k1,
+                                               acc, bad);
         }
         // Layers k0..k1-1 are complete: hTr(knat) += dTr(knat) * (1/areaT), knat = nz + 1 - k.
 #pragma unroll

@@ -227,6 +227,7 @@ struct CellTuning {
     int flux_staged = 0;  // face flux with its reconstruction loads staged one sublayer ahead (groups <= 2)
     int gather_batch = 0;  // shared-memory gather: sublayers per round trip (8, or 0: 3 / 4 by chunk)
     int sweep_form = 4;    // neutral sweep: 0 register windows, 3 / 4 / 5 windows in a shared-memory ring of that size
+    int gather_pipe = 0;   // shared-memory gather: batches of 4 software-pipelined (the next one in flight)
 };
 CellTuning cell_tuning();
 void set_cell_tuning(const CellTuning& t);

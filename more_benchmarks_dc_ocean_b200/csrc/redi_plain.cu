@@ -146,7 +146,8 @@ __global__ void __launch_bounds__(128) k_cell_gather(CellGatherArgsT<P> a, int t
 
 // The gather with its per-layer sums in shared memory (gather_item_s).
 // U: sublayers fetched per round trip (0: 3 for 4-layer chunks, 4 otherwise).
-template <int NT, int CH, class P, int U = 0>
+// PIPE: the walk's batches software-pipelined (gather_run_sp).
+template <int NT, int CH, class P, int U = 0, bool PIPE = false>
 __global__ void __launch_bounds__(kGatherThreads) k_cell_gather_s(CellGatherArgsT<P> a, int tr0, int fslot, int j0,
                                                                   int j1) {
     __shared__ double acc[CH * NT * kGatherThreads];
@@ -154,7 +155,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_cell_gather_s(CellGatherArgs
     const int j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
     constexpr int kU = U ? U : (CH <= 4 ? 3 : 4);
     if (j < j1)
-        gather_item_s<NT, CH, P, LdNC, kU>(a, blockIdx.x * blockDim.x + threadIdx.x, j, tr0, fslot, acc + tid);
+        gather_item_s<NT, CH, P, LdNC, kU, PIPE>(a, blockIdx.x * blockDim.x + threadIdx.x, j, tr0, fslot, acc + tid);
 }
 
 // The point EOS at n independent points, as the column state evaluates it at
@@ -282,6 +283,18 @@ static void launch_gather(const CellGatherArgsT<P>& cg, int tr, int slot, const 
     // shared-memory sums: CH x GNT x 128 doubles must stay within the 48 KB of static shared memory
     if (tune.gather_smem && block.x * block.y == plain::kGatherThreads && tune.chunk * GNT <= 32) {
         const bool deep = tune.gather_batch >= 8;  // 8 sublayers per round trip instead of 3-4
+        if (tune.gather_pipe) {  // batches of 4, the next one in flight
+            switch (tune.chunk) {
+                case 4: plain::k_cell_gather_s<GNT, 4, P, 4, true><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1); break;
+                case 16:
+                    if constexpr (GNT <= 2)
+                        plain::k_cell_gather_s<GNT, 16, P, 4, true><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1);
+                    break;
+                default: plain::k_cell_gather_s<GNT, 8, P, 4, true><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1); break;
+            }
+            launch_end(K_CELL_UPDATE, st);
+            return;
+        }
         switch (tune.chunk) {
             case 4:
                 if (deep) plain::k_cell_gather_s<GNT, 4, P, 8><<<cgrid, block, 0, st>>>(cg, tr, slot, r.j0, r.j1);

@@ -282,7 +282,8 @@ def test_mixed_precision_many_tracers_and_gates(redi_lib, oracle_lib):
 
 
 @pytest.mark.parametrize("gnt,smem,chunk", [(2, 1, 4), (2, 1, 8), (2, 1, 16), (4, 0, 4), (4, 1, 8), (2, 2, 8),
-                                            (2, 2, 16), (4, 2, 4), (8, 1, 4), (8, 2, 4), (8, 1, 8)])
+                                            (2, 2, 16), (4, 2, 4), (8, 1, 4), (8, 2, 4), (8, 1, 8), (2, 3, 4),
+                                            (2, 3, 8), (2, 3, 16), (4, 3, 4), (4, 3, 8)])
 def test_gather_forms_match_oracle(redi_lib, oracle_lib, gnt, smem, chunk):
     """The gather folding 2, 4 or 8 tracers per launch (8: two face-flux launches of 4 into one
     flux buffer; with 8-layer chunks it falls back to 4), with its per-layer sums in registers or
